@@ -1,0 +1,543 @@
+// DFSPH sweeps of the DIMCV-SPH substep (reference: DIMCVSPHSolver /
+// SPHBase, dimcv_sph.py:86-226, 337-614; sph_base.py:91-112).  One thread
+// per particle slot in the cell-sorted order; each per-pair expression keeps
+// the reference's operation order (compiled with -fmad=false, IEEE div/sqrt).
+// The Jacobi loops run on the device: every iteration kernel returns at once
+// when the solve's done flag is set, so the host launches iterations in
+// chunks and polls the flag once per chunk instead of once per iteration.
+#include <algorithm>
+
+#include "dv_internal.cuh"
+
+#define FOR_I                                      \
+  int i = blockIdx.x * blockDim.x + threadIdx.x;   \
+  if (i >= C->n) return;
+
+// --------------------------------------------------------- boundary volume
+// compute_static_boundary_volume (sph_base.py:91-103)
+template <int D>
+__global__ void k_boundary_volume(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (!(F.material[i] == DV_MATERIAL_SOLID && !F.is_dynamic[i])) return;
+  V3 xi = ldv<D>(F.x, i);
+  float delta = cubic_W(P, 0.0f);
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3, float r2) {
+    if (F.material[j] == DV_MATERIAL_SOLID) delta += cubic_W(P, sqrtf(r2));
+  });
+  F.m_V[i] = 1.0f / delta * 3.0f;
+}
+
+// ---------------------------------------------------------------- density
+// compute_densities (dimcv_sph.py:126-148)
+template <int D>
+__global__ void k_densities(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (F.material[i] != DV_MATERIAL_FLUID) return;
+  V3 xi = ldv<D>(F.x, i);
+  float dens = F.m_V[i] * cubic_W(P, 0.0f);
+  float den = 0.0f;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) den += F.m_V[j] * cubic_W(P, sqrtf(r2));
+  });
+  dens += den;
+  dens *= P.density0;
+  F.density[i] = dens;
+}
+
+// ---------------------------------------------------------- DFSPH factor
+// compute_DFSPH_factor (dimcv_sph.py:86-124)
+template <int D>
+__global__ void k_dfsph_factor(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (F.material[i] != DV_MATERIAL_FLUID) return;
+  V3 xi = ldv<D>(F.x, i);
+  V3 gi{0.f, 0.f, 0.f};
+  float sum_k = 0.0f;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID) {
+      V3 gw = cubic_gradW<D>(P, r, r2);
+      float mm = F.m[j];
+      V3 g{mm * gw.x, mm * gw.y, mm * gw.z};
+      sum_k += sqnorm<D>(g);
+      gi.x += g.x;
+      gi.y += g.y;
+      if (D == 3) gi.z += g.z;
+    } else if (mj == DV_MATERIAL_SOLID) {
+      V3 gw = cubic_gradW<D>(P, r, r2);
+      float s = F.m_V[j] * P.density0;
+      gi.x += s * gw.x;
+      gi.y += s * gw.y;
+      if (D == 3) gi.z += s * gw.z;
+    }
+  });
+  sum_k += sqnorm<D>(gi);
+  F.dfsph_factor[i] = sum_k > P.factor_min ? 1.0f / sum_k : 0.0f;
+}
+
+// multiply_time_step (dimcv_sph.py:395-399)
+__global__ void k_scale_factor(dv_fields F, float s, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (F.material[i] == DV_MATERIAL_FLUID) F.dfsph_factor[i] *= s;
+}
+
+// ------------------------------------------------------- density change
+// compute_density_change (dimcv_sph.py:337-374); optionally the block
+// partial of compute_density_error(0) (dimcv_sph.py:407-419) in FP64.
+template <int D>
+__global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                 const int32_t* __restrict__ done, double* __restrict__ part) {
+  if (done && *done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+    V3 xi = ldv<D>(F.x, i);
+    V3 vi = ldv<D>(F.v, i);
+    float adv = 0.0f;
+    int nn = 0;
+    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+      int mj = F.material[j];
+      if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
+        V3 vj = ldv<D>(F.v, j);
+        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+        adv += F.m_V[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+      }
+      nn += 1;
+    });
+    float da = fmaxf(adv, 0.0f);
+    if (nn < P.neighbor_min) da = 0.0f;
+    F.density_adv[i] = da;
+    if (part) {
+      float term = P.has_transit ? transit_weight(P, xi.x) * (da - 0.0f) : (da - 0.0f);
+      err = (double)term;
+    }
+  }
+  if (part) {
+    double s = block_sum<double>(err);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+  }
+}
+
+// ------------------------------------------------------------ density adv
+// compute_density_adv (dimcv_sph.py:470-493); optionally the block partial of
+// compute_density_error(density0).
+template <int D>
+__global__ void k_density_adv(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                              const int32_t* __restrict__ done, double* __restrict__ part) {
+  if (done && *done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+    V3 xi = ldv<D>(F.x, i);
+    V3 vi = ldv<D>(F.v, i);
+    float delta = 0.0f;
+    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+      int mj = F.material[j];
+      if (mj == DV_MATERIAL_FLUID) {
+        V3 vj = ldv<D>(F.v, j);
+        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+        delta += F.m[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+      } else if (mj == DV_MATERIAL_SOLID) {
+        V3 vj = ldv<D>(F.v, j);
+        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+        delta += F.m_V[j] * P.density0 * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+      }
+    });
+    float da = F.density[i] + P.dt * delta;
+    da = fmaxf(da, P.density0);
+    F.density_adv[i] = da;
+    if (part) {
+      float term = P.has_transit ? transit_weight(P, xi.x) * (da - P.density0) : (da - P.density0);
+      err = (double)term;
+    }
+  }
+  if (part) {
+    double s = block_sum<double>(err);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+  }
+}
+
+// compute_density_error without a preceding sweep (operator surface)
+template <int D>
+__global__ void k_density_error(dv_params P, dv_fields F, const dv_counters* __restrict__ C,
+                                float offset, double* __restrict__ part) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+    float da = F.density_adv[i];
+    float term;
+    if (P.has_transit) {
+      V3 xi = ldv<D>(F.x, i);
+      term = transit_weight(P, xi.x) * (da - offset);
+    } else {
+      term = da - offset;
+    }
+    err = (double)term;
+  }
+  double s = block_sum<double>(err);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// ---------------------------------------------------- Jacobi iterations
+// divergence_solver_iteration_kernel (dimcv_sph.py:421-468)
+template <int D>
+__global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                  const int32_t* __restrict__ done) {
+  if (done && *done) return;
+  FOR_I;
+  if (F.material[i] != DV_MATERIAL_FLUID) return;
+  V3 xi = ldv<D>(F.x, i);
+  float b_i = F.density_adv[i];
+  float k_i = b_i * F.dfsph_factor[i] * F.density[i];
+  V3 dv{0.f, 0.f, 0.f};
+  const float dt = P.dt;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID) {
+      float b_j = F.density_adv[j];
+      float k_j = b_j * F.dfsph_factor[j] * F.density[j];
+      float k_sum = k_i + k_j;
+      if (fabsf(k_sum) > P.m_eps) {
+        V3 gw = cubic_gradW<D>(P, r, r2);
+        float mm = F.m[j];
+        float s = dt * k_sum;
+        dv.x -= s * (mm * gw.x);
+        dv.y -= s * (mm * gw.y);
+        if (D == 3) dv.z -= s * (mm * gw.z);
+      }
+    } else if (mj == DV_MATERIAL_SOLID) {
+      if (fabsf(k_i) > P.m_eps) {
+        V3 gw = cubic_gradW<D>(P, r, r2);
+        float sm = F.m_V[j] * P.density0;
+        float s = -dt * 1.0f * k_i;
+        dv.x += s * (sm * gw.x);
+        dv.y += s * (sm * gw.y);
+        if (D == 3) dv.z += s * (sm * gw.z);
+      }
+    }
+  });
+  V3 vi = ldv<D>(F.v, i);
+  if (P.has_transit) {
+    float w = transit_weight(P, xi.x);
+    vi.x += w * dv.x;
+    vi.y += w * dv.y;
+    if (D == 3) vi.z += w * dv.z;
+  } else {
+    vi.x += dv.x;
+    vi.y += dv.y;
+    if (D == 3) vi.z += dv.z;
+  }
+  stv<D>(F.v, i, vi);
+}
+
+// pressure_solve_iteration_kernel (dimcv_sph.py:495-549): the velocity is
+// updated pair by pair (the reference writes v[p_i] inside the task).
+template <int D>
+__global__ void k_pressure_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                const int32_t* __restrict__ done) {
+  if (done && *done) return;
+  FOR_I;
+  if (F.material[i] != DV_MATERIAL_FLUID) return;
+  V3 xi = ldv<D>(F.x, i);
+  V3 vi = ldv<D>(F.v, i);
+  float b_i = F.density_adv[i] - P.density0;
+  float k_i = b_i * F.dfsph_factor[i];
+  const float dt = P.dt;
+  const float w = P.has_transit ? transit_weight(P, xi.x) : 1.0f;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID) {
+      float b_j = F.density_adv[j] - P.density0;
+      float k_j = b_j * F.dfsph_factor[j];
+      float k_sum = k_i + k_j;
+      if (fabsf(k_sum) > P.m_eps) {
+        V3 gw = cubic_gradW<D>(P, r, r2);
+        float mm = F.m[j];
+        float s = P.has_transit ? (w * dt) * k_sum : dt * k_sum;
+        vi.x -= s * (mm * gw.x);
+        vi.y -= s * (mm * gw.y);
+        if (D == 3) vi.z -= s * (mm * gw.z);
+      }
+    } else if (mj == DV_MATERIAL_SOLID) {
+      if (fabsf(k_i) > P.m_eps) {
+        V3 gw = cubic_gradW<D>(P, r, r2);
+        float sm = F.m_V[j] * P.density0;
+        float s = -dt * 1.0f * k_i;
+        V3 vc{s * (sm * gw.x), s * (sm * gw.y), D == 3 ? s * (sm * gw.z) : 0.0f};
+        if (P.has_transit) {
+          vi.x += w * vc.x;
+          vi.y += w * vc.y;
+          if (D == 3) vi.z += w * vc.z;
+        } else {
+          vi.x += vc.x;
+          vi.y += vc.y;
+          if (D == 3) vi.z += vc.z;
+        }
+      }
+    }
+  });
+  stv<D>(F.v, i, vi);
+}
+
+// convergence test of one Jacobi iteration: average error over the fluid
+// count against eta; sets the done flag at convergence or at max_iter
+__global__ void k_solve_finalize(const double* __restrict__ part, int nparts, dv_counters* C,
+                                 int32_t* done, double eta, int max_iter, int which) {
+  if (*done) return;
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nparts; k += blockDim.x) s += part[k];
+  s = block_sum<double>(s);
+  if (threadIdx.x == 0) {
+    int nf = C->n_fluid;
+    double avg = nf > 0 ? s / (double)nf : 0.0;
+    int it = (which == 0 ? ++C->iters_div : ++C->iters_p);
+    if (which == 0)
+      C->err_div = avg;
+    else
+      C->err_p = avg;
+    if (!isfinite(avg)) C->status |= DV_WARN_NAN;
+    if (avg <= eta || nf == 0) {
+      *done = 1;
+    } else if (it >= max_iter) {
+      *done = 1;
+      C->status |= (which == 0 ? DV_WARN_DIV_NOT_CONVERGED : DV_WARN_P_NOT_CONVERGED);
+    }
+  }
+}
+
+__global__ void k_solve_reset(dv_counters* C, int32_t* done, int which) {
+  *done = 0;
+  if (which == 0)
+    C->iters_div = 0;
+  else
+    C->iters_p = 0;
+}
+
+// ------------------------------------------------------- non-pressure forces
+// compute_non_pressure_forces (dimcv_sph.py:150-208).  The surface tension
+// coefficient is 0 in the reference (dimcv_sph.py:12) and boundary viscosity
+// is 0 (:182), so those terms add exactly zero and are not evaluated.
+template <int D>
+__global__ void k_nonpressure(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  int mi = F.material[i];
+  if (mi == DV_MATERIAL_SOLID && !F.is_dynamic[i]) {
+    stv<D>(F.acceleration, i, V3{0.f, 0.f, 0.f});
+    return;
+  }
+  V3 dv{P.gravity[0], P.gravity[1], D == 3 ? P.gravity[2] : 0.0f};
+  if (mi == DV_MATERIAL_FLUID) {
+    V3 xi = ldv<D>(F.x, i);
+    V3 vi = ldv<D>(F.v, i);
+    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+      if (F.material[j] == DV_MATERIAL_FLUID) {
+        V3 vj = ldv<D>(F.v, j);
+        V3 dvij{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+        float v_xy = dot<D>(dvij, r);
+        float rn = sqrtf(r2);
+        float s = P.visc_coef * F.m_V[j] * v_xy / (rn * rn + P.visc_h2);
+        V3 gw = cubic_gradW<D>(P, r, r2);
+        dv.x += s * gw.x;
+        dv.y += s * gw.y;
+        if (D == 3) dv.z += s * gw.z;
+      }
+    });
+  }
+  stv<D>(F.acceleration, i, dv);
+}
+
+// predict_velocity (dimcv_sph.py:220-226)
+template <int D>
+__global__ void k_predict_velocity(dv_params P, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (!(F.is_dynamic[i] && F.material[i] == DV_MATERIAL_FLUID)) return;
+  V3 v = ldv<D>(F.v, i), a = ldv<D>(F.acceleration, i);
+  v.x += P.dt * a.x;
+  v.y += P.dt * a.y;
+  if (D == 3) v.z += P.dt * a.z;
+  stv<D>(F.v, i, v);
+}
+
+// advect (dimcv_sph.py:210-218)
+template <int D>
+__global__ void k_advect(dv_params P, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (!F.is_dynamic[i]) return;
+  V3 v = ldv<D>(F.v, i);
+  if (F.material[i] == DV_MATERIAL_SOLID) {
+    V3 a = ldv<D>(F.acceleration, i);
+    v.x += P.dt * a.x;
+    v.y += P.dt * a.y;
+    if (D == 3) v.z += P.dt * a.z;
+    stv<D>(F.v, i, v);
+  }
+  V3 x = ldv<D>(F.x, i);
+  x.x += P.dt * v.x;
+  x.y += P.dt * v.y;
+  if (D == 3) x.z += P.dt * v.z;
+  stv<D>(F.x, i, x);
+}
+
+// ------------------------------------------------------------- host side
+#define LAUNCH_D(kern, nb, ...)                                                          \
+  do {                                                                                   \
+    if (c->p.dim == 2)                                                                   \
+      kern<2><<<(nb), DV_THREADS, 0, c->stream>>>(__VA_ARGS__);                          \
+    else                                                                                 \
+      kern<3><<<(nb), DV_THREADS, 0, c->stream>>>(__VA_ARGS__);                          \
+    DV_LAUNCHED(c);                                                                      \
+  } while (0)
+
+static inline int nblk(const dv_ctx* c) { return dv_blocks(std::min<int64_t>(c->n_upper, c->cap)); }
+
+DV_API int dv_boundary_volume(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_densities(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_densities, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_dfsph_factor(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_dfsph_factor, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_scale_factor(dv_ctx* c, const dv_fields* f, float s) {
+  if (!c || !f) return DV_EINVAL;
+  k_scale_factor<<<nblk(c), DV_THREADS, 0, c->stream>>>(*f, s, c->d_cnt);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+DV_API int dv_density_change(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_density_change, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
+           (double*)nullptr);
+  return DV_OK;
+}
+
+DV_API int dv_density_adv(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_density_adv, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
+           (double*)nullptr);
+  return DV_OK;
+}
+
+DV_API int dv_density_error(dv_ctx* c, const dv_fields* f, float offset, double* out) {
+  if (!c || !f || !out) return DV_EINVAL;
+  int nb = nblk(c);
+  LAUNCH_D(k_density_error, nb, c->p, *f, c->d_cnt, offset, c->red_part);
+  double* dst = reinterpret_cast<double*>(c->dscan_part);  // scratch word
+  int rc = dv_finalize_sum(c, c->red_part, nb, dst);
+  if (rc) return rc;
+  DV_CK(c, cudaMemcpyAsync(out, dst, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DV_CK(c, cudaStreamSynchronize(c->stream));
+  return DV_OK;
+}
+
+DV_API int dv_divergence_iteration(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_divergence_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
+  return DV_OK;
+}
+
+DV_API int dv_pressure_iteration(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
+  return DV_OK;
+}
+
+// Runs Jacobi iterations in chunks of 2, 4, 8, ... launches; every iteration
+// is (update sweep, residual sweep + FP64 block partials, finalize) and all
+// three return at once once the done flag is set.
+static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
+  const int nb = nblk(c);
+  const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
+  const double eta = which == 0 ? c->p.eta_div : c->p.eta_p;
+  int32_t* done = c->d_flag;
+  k_solve_reset<<<1, 1, 0, c->stream>>>(c->d_cnt, done, which);
+  DV_LAUNCHED(c);
+  int launched = 0, chunk = 2;
+  while (launched < max_iter) {
+    int m = std::min(chunk, max_iter - launched);
+    for (int k = 0; k < m; ++k) {
+      if (which == 0) {
+        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
+        LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                 c->red_part);
+      } else {
+        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
+        LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                 c->red_part);
+      }
+      k_solve_finalize<<<1, 1024, 0, c->stream>>>(c->red_part, nb, c->d_cnt, done, eta, max_iter,
+                                                  which);
+      DV_LAUNCHED(c);
+    }
+    launched += m;
+    if (launched >= max_iter) break;
+    DV_CK(c, cudaMemcpyAsync(c->h_flag, done, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DV_CK(c, cudaStreamSynchronize(c->stream));
+    if (*c->h_flag) break;
+    chunk *= 2;
+  }
+  return DV_OK;
+}
+
+static int read_iters(dv_ctx* c, int which, int32_t* iters) {
+  if (!iters) return DV_OK;
+  dv_counters cnt;
+  int rc = dv_get_counters(c, &cnt);
+  if (rc) return rc;
+  *iters = which == 0 ? cnt.iters_div : cnt.iters_p;
+  return DV_OK;
+}
+
+DV_API int dv_divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  int rc = dv_density_change(c, f);
+  if (rc) return rc;
+  rc = dv_scale_factor(c, f, c->p.inv_dt);
+  if (rc) return rc;
+  rc = jacobi_loop(c, f, 0);
+  if (rc) return rc;
+  rc = dv_scale_factor(c, f, c->p.dt);
+  if (rc) return rc;
+  return read_iters(c, 0, iters);
+}
+
+DV_API int dv_pressure_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  int rc = dv_density_adv(c, f);
+  if (rc) return rc;
+  rc = dv_scale_factor(c, f, c->p.inv_dt2);
+  if (rc) return rc;
+  rc = jacobi_loop(c, f, 1);
+  if (rc) return rc;
+  return read_iters(c, 1, iters);
+}
+
+DV_API int dv_nonpressure(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_nonpressure, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_predict_velocity(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_predict_velocity, nblk(c), c->p, *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_advect(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_advect, nblk(c), c->p, *f, c->d_cnt);
+  return DV_OK;
+}

@@ -1,0 +1,446 @@
+// N-body parts of the VVPE (reference: DIMCVSPHSolver.vort2vel,
+// dimcv_sph.py:679-719) and the full Biot-Savart comparator.  These are
+// FP32-pipe bound: each CTA stages tiles of sources (position, weighted
+// vorticity) in shared memory and every thread accumulates TT targets in
+// registers, so one broadcast shared load feeds TT pair evaluations.
+//
+// Far-field pair (reference kernel): the sample counts iff
+// sqrtf(|r|²) > h, tested exactly as r2 > far_r2_limit with r2 summed in the
+// reference order without FMA; Kε(|r|) = 1/(|r|·|r|) there because
+// exp(-|r|/ε) underflows to 0 for |r| > h >= 1.05e-4 (checked on the host,
+// otherwise the exact regularised form is used).  The sample's 1/(kden+1e-8)
+// and the target's (kden_sum - S_i) are folded out of the pair loop.
+// This file is compiled with FMA contraction on.
+#include <algorithm>
+
+#include "dv_internal.cuh"
+
+int dv_build_targets(dv_ctx* c, const dv_fields* f);
+int dv_launch_vvpe_near(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s);
+
+#define FT 256  // threads per CTA
+#define FTILE 256
+
+// ------------------------------------------------------------ sample pack
+// spos = (x, y, z|0, 0), sw = ω̃ / (kden + 1e-8)  (dimcv_sph.py:706-709)
+template <int D>
+__global__ void k_pack_samples(const dv_fields F, const dv_solver_fields S,
+                               const dv_counters* __restrict__ C, float4* __restrict__ spos,
+                               float4* __restrict__ sw, float kden_eps) {
+  const int M = C->num_samples;
+  const int n = C->n;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < M; s += gridDim.x * blockDim.x) {
+    int j = S.sample_idx[s];
+    if (j < 0 || j >= n) {  // a caller-injected index outside [0, n): no contribution
+      atomicOr(const_cast<int32_t*>(&C->status), DV_WARN_BAD_INDEX);
+      spos[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      sw[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
+    }
+    V3 x = ldv<D>(F.x, j);
+    V3 w = ld4(S.d_vort_smoothed, j);
+    float inv = 1.0f / (S.kden[j] + kden_eps);
+    spos[s] = make_float4(x.x, x.y, x.z, 0.0f);
+    sw[s] = make_float4(w.x * inv, w.y * inv, w.z * inv, 0.0f);
+  }
+}
+
+template <bool COMP>
+struct Acc {
+  float s = 0.0f, c = 0.0f;
+  __device__ __forceinline__ void add(float t) {
+    if (COMP) {  // Kahan: y = t - c; u = s + y; c = (u - s) - y; s = u
+      float y = __fsub_rn(t, c);
+      float u = __fadd_rn(s, y);
+      c = __fsub_rn(__fsub_rn(u, s), y);
+      s = u;
+    } else {
+      s += t;
+    }
+  }
+  __device__ __forceinline__ float val() const { return COMP ? __fsub_rn(s, c) : s; }
+};
+
+// Regularised reference kernel Kε(r) for r2 below the underflow bound.
+__device__ __forceinline__ float k_eps_exact(const dv_params& P, float r2) {
+  float rn = sqrtf(r2);
+  float e = expf(-rn * P.inv_eps);
+  return (1.0f - e) / (rn * (rn + P.eps * e));
+}
+
+template <int D, int TT, bool BLOB, bool COMP, bool FASTK>
+__global__ void __launch_bounds__(FT) k_vvpe_far(dv_params P, dv_fields F, dv_solver_fields S,
+                                                 const dv_counters* __restrict__ C,
+                                                 const int32_t* __restrict__ targets,
+                                                 const float4* __restrict__ spos,
+                                                 const float4* __restrict__ sw,
+                                                 const float4* __restrict__ near_v,
+                                                 const float* __restrict__ near_S) {
+  __shared__ float4 s_p[FTILE];
+  __shared__ float4 s_w[FTILE];
+  const int nt = C->n_targets;
+  const int M = C->num_samples;
+  const int tbase = blockIdx.x * FT * TT;
+  if (tbase >= nt) return;  // uniform per CTA
+  float px[TT], py[TT], pz[TT];
+  Acc<COMP> ax[TT], ay[TT], az[TT];
+  int cnt[TT];
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT + threadIdx.x;
+    int i = targets[t < nt ? t : nt - 1];
+    V3 x = ldv<D>(F.x, i);
+    px[k] = x.x;
+    py[k] = x.y;
+    pz[k] = x.z;
+    cnt[k] = 0;
+  }
+  const float lim = P.far_r2_limit;
+  const float d2 = P.blob_delta2;
+  for (int base = 0; base < M; base += FTILE) {
+    const int m = min(FTILE, M - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT) {
+      s_p[q] = spos[base + q];
+      s_w[q] = sw[base + q];
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int q = 0; q < m; ++q) {
+      const float4 sp = s_p[q];
+      const float4 w = s_w[q];
+#pragma unroll
+      for (int k = 0; k < TT; ++k) {
+        float dx = __fsub_rn(px[k], sp.x);
+        float dy = __fsub_rn(py[k], sp.y);
+        float dz = D == 3 ? __fsub_rn(pz[k], sp.z) : 0.0f;
+        float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        if (D == 3) r2 = __fadd_rn(r2, __fmul_rn(dz, dz));
+        const bool far = r2 > lim;
+        cnt[k] += far ? 1 : 0;
+        if (!BLOB) {
+          float kk;
+          if (FASTK)
+            kk = far ? __fdividef(1.0f, r2) : 0.0f;
+          else
+            kk = far ? k_eps_exact(P, r2) : 0.0f;
+          // K (r_xy × w) with r_xy = (dx, dy, 0)
+          float t = kk * w.z;
+          ax[k].add(t * dy);
+          ay[k].add(-t * dx);
+          az[k].add(kk * (dx * w.y - dy * w.x));
+        } else {
+          float s = r2 + d2;
+          float inv = rsqrtf(s);
+          float kk = far ? inv * inv * inv : 0.0f;
+          ax[k].add(kk * (dy * w.z - dz * w.y));
+          ay[k].add(kk * (dz * w.x - dx * w.z));
+          az[k].add(kk * (dx * w.y - dy * w.x));
+        }
+      }
+    }
+  }
+  const float coef = BLOB ? P.blob_coef : P.vvpe_coef;
+  const float kden_sum = C->kden_sum_f32;
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT + threadIdx.x;
+    if (t >= nt) continue;
+    int i = targets[t];
+    float4 nv = near_v[t];
+    float fac = kden_sum - near_S[t];
+    V3 fv{0.f, 0.f, 0.f};
+    if (cnt[k] > 0) {
+      float sc = coef / (float)cnt[k];
+      fv.x = (ax[k].val() * fac) * sc;
+      fv.y = (ay[k].val() * fac) * sc;
+      fv.z = (az[k].val() * fac) * sc;
+    }
+    V3 vv{fv.x + nv.x, fv.y + nv.y, fv.z + nv.z};
+    if (S.v_vort) st4(S.v_vort, i, vv);
+    // gate ‖v_vort‖ < ‖v_i‖ (dimcv_sph.py:717-719)
+    float n1 = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vv.x, vv.x), __fmul_rn(vv.y, vv.y)),
+                               __fmul_rn(vv.z, vv.z)));
+    V3 vi = ldv<D>(F.v, i);
+    float n2 = sqrtf(sqnorm<D>(vi));
+    if (n1 < n2) {
+      vi.x = __fadd_rn(vi.x, vv.x);
+      vi.y = __fadd_rn(vi.y, vv.y);
+      if (D == 3) vi.z = __fadd_rn(vi.z, vv.z);
+      stv<D>(F.v, i, vi);
+    }
+  }
+}
+
+template <int D, int TT, bool BLOB, bool COMP, bool FASTK>
+static void launch_far(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, int nb) {
+  k_vvpe_far<D, TT, BLOB, COMP, FASTK><<<nb, FT, 0, c->stream>>>(
+      c->p, *f, *s, c->d_cnt, c->targets, c->spos, c->sw, c->near_v, c->near_S);
+}
+
+template <int D>
+static void dispatch_far(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, int nb, bool fastk) {
+  constexpr int TT = 2;
+  const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  const bool comp = c->p.compensated != 0;
+  if (blob) {
+    if (comp)
+      launch_far<D, TT, true, true, true>(c, f, s, nb);
+    else
+      launch_far<D, TT, true, false, true>(c, f, s, nb);
+  } else if (fastk) {
+    if (comp)
+      launch_far<D, TT, false, true, true>(c, f, s, nb);
+    else
+      launch_far<D, TT, false, false, true>(c, f, s, nb);
+  } else {
+    if (comp)
+      launch_far<D, TT, false, true, false>(c, f, s, nb);
+    else
+      launch_far<D, TT, false, false, false>(c, f, s, nb);
+  }
+}
+
+// exp(-h/ε) underflows to zero in f32 once h/ε > 103.97
+static bool fast_kernel_ok(const dv_params& P) {
+  return (double)P.support_radius * (double)P.inv_eps > 104.5;
+}
+
+__global__ void k_prof_pairs(const dv_counters* __restrict__ C, double* acc) {
+  acc[0] += (double)C->n_targets * (double)C->num_samples;
+}
+
+static int prof_fold(dv_ctx* c) {
+  for (int k = 0; k < c->prof_used; ++k) {
+    float ms = 0.f;
+    DV_CK(c, cudaEventSynchronize(c->prof_ev[2 * k + 1]));
+    DV_CK(c, cudaEventElapsedTime(&ms, c->prof_ev[2 * k], c->prof_ev[2 * k + 1]));
+    c->prof_ms += ms;
+  }
+  c->prof_used = 0;
+  return DV_OK;
+}
+
+DV_API int dv_profile(dv_ctx* c, int32_t enable) {
+  if (!c) return DV_EINVAL;
+  int rc = prof_fold(c);
+  if (rc) return rc;
+  if (enable && !c->prof_ev[0])
+    for (int k = 0; k < 2 * dv_ctx::kProfPool; ++k) DV_CK(c, cudaEventCreate(&c->prof_ev[k]));
+  c->prof = enable != 0;
+  c->prof_ms = 0.0;
+  c->prof_launches = 0;
+  DV_CK(c, cudaMemsetAsync(c->d_prof, 0, sizeof(double) * 4, c->stream));
+  return DV_OK;
+}
+
+DV_API int dv_profile_read(dv_ctx* c, double* far_ms, int64_t* launches, double* pairs) {
+  if (!c) return DV_EINVAL;
+  int rc = prof_fold(c);
+  if (rc) return rc;
+  double h[4];
+  DV_CK(c, cudaMemcpyAsync(h, c->d_prof, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+  DV_CK(c, cudaStreamSynchronize(c->stream));
+  if (far_ms) *far_ms = c->prof_ms;
+  if (launches) *launches = c->prof_launches;
+  if (pairs) *pairs = h[0];
+  return DV_OK;
+}
+
+DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
+  if (!c || !f || !s || !s->sample_idx || !s->kden || !s->d_vort_smoothed)
+    return c ? dv_fail(c, DV_EINVAL, "dv_vvpe_mc: NULL field") : DV_EINVAL;
+  int rc = dv_build_targets(c, f);
+  if (rc) return rc;
+  rc = dv_launch_vvpe_near(c, f, s);
+  if (rc) return rc;
+  const int packb = c->num_sms * 4;
+  if (c->p.dim == 2)
+    k_pack_samples<2><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw,
+                                                          c->p.kden_eps);
+  else
+    k_pack_samples<3><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw,
+                                                          c->p.kden_eps);
+  DV_LAUNCHED(c);
+  const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
+  const int nb = (int)std::max<int64_t>(1, (nu + FT * 2 - 1) / (FT * 2));
+  const bool fastk = fast_kernel_ok(c->p);
+  if (c->prof) {
+    if (c->prof_used == dv_ctx::kProfPool) {
+      int rc2 = prof_fold(c);
+      if (rc2) return rc2;
+    }
+    DV_CK(c, cudaEventRecord(c->prof_ev[2 * c->prof_used], c->stream));
+  }
+  if (c->p.dim == 2)
+    dispatch_far<2>(c, f, s, nb, fastk);
+  else
+    dispatch_far<3>(c, f, s, nb, fastk);
+  DV_LAUNCHED(c);
+  if (c->prof) {
+    DV_CK(c, cudaEventRecord(c->prof_ev[2 * c->prof_used + 1], c->stream));
+    c->prof_used++;
+    c->prof_launches++;
+    k_prof_pairs<<<1, 1, 0, c->stream>>>(c->d_cnt, c->d_prof);
+    DV_LAUNCHED(c);
+  }
+  return DV_OK;
+}
+
+// ------------------------------------------------------------ full BS
+// sources: fluid slots in ascending order, (x, y, z, slot bits) and ω
+template <int D>
+__global__ void k_flag_fluid(const dv_fields F, const dv_counters* __restrict__ C, int m,
+                             uint32_t* __restrict__ flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  flags[i] = (i < C->n && F.material[i] == DV_MATERIAL_FLUID) ? 1u : 0u;
+}
+
+template <int D>
+__global__ void k_pack_sources(const dv_fields F, const float* __restrict__ omega,
+                               const uint32_t* __restrict__ flags, const uint32_t* __restrict__ offs,
+                               const dv_counters* __restrict__ C, float4* __restrict__ spos,
+                               float4* __restrict__ sw, int32_t* __restrict__ ns_out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = C->n;
+  if (i == 0) *ns_out = (int32_t)offs[n];
+  if (i >= n || !flags[i]) return;
+  uint32_t q = offs[i];
+  V3 x = ldv<D>(F.x, i);
+  float4 w = reinterpret_cast<const float4*>(omega)[i];
+  spos[q] = make_float4(x.x, x.y, x.z, __int_as_float(i));
+  sw[q] = make_float4(w.x, w.y, w.z, 0.0f);
+}
+
+// Σ_{j fluid, j != i} kernel(r_ij) (r × ω_j) for target slots; T = float or
+// double (the FP64 comparator).  Reference kernel: Kε(|r|) (r_xy × ω), with
+// the exact regularised form where exp(-|r|/ε) does not underflow and a zero
+// contribution from coincident pairs (the limit of Kε(r) r as r -> 0).
+template <int D, typename T, bool BLOB>
+__global__ void __launch_bounds__(FT) k_bs_full(dv_params P, const float* __restrict__ x,
+                                                const int32_t* __restrict__ tlist, int nt,
+                                                const float4* __restrict__ spos,
+                                                const float4* __restrict__ sw,
+                                                const int32_t* __restrict__ ns_p, const dv_counters* __restrict__ C,
+                                                T* __restrict__ out) {
+  __shared__ float4 s_p[FTILE];
+  __shared__ float4 s_w[FTILE];
+  const int ns = *ns_p;
+  const int t = blockIdx.x * FT + threadIdx.x;
+  int i = t < nt ? (tlist ? tlist[t] : t) : -1;
+  if (t < nt && (i < 0 || i >= C->n)) {  // caller target outside [0, n): zero output
+    out[(int64_t)t * 4 + 0] = 0;
+    out[(int64_t)t * 4 + 1] = 0;
+    out[(int64_t)t * 4 + 2] = 0;
+    out[(int64_t)t * 4 + 3] = 0;
+    i = -1;
+  }
+  T px = 0, py = 0, pz = 0;
+  if (i >= 0) {
+    V3 xi = ldv<D>(x, i);
+    px = (T)xi.x;
+    py = (T)xi.y;
+    pz = (T)xi.z;
+  }
+  T ax = 0, ay = 0, az = 0;
+  const T eps = (T)P.eps, inv_eps = (T)P.inv_eps, d2 = (T)P.blob_delta2;
+  // exp(-|r|/ε) underflows below these |r|² bounds (f32: 104 ε, f64: 746 ε)
+  const T under = sizeof(T) == 4 ? (T)(104.5 * 104.5) * eps * eps : (T)(746.0 * 746.0) * eps * eps;
+  for (int base = 0; base < ns; base += FTILE) {
+    const int m = min(FTILE, ns - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT) {
+      s_p[q] = spos[base + q];
+      s_w[q] = sw[base + q];
+    }
+    __syncthreads();
+    if (i < 0) continue;
+    for (int q = 0; q < m; ++q) {
+      const float4 sp = s_p[q];
+      if (__float_as_int(sp.w) == i) continue;
+      const float4 w = s_w[q];
+      T dx = px - (T)sp.x, dy = py - (T)sp.y, dz = D == 3 ? pz - (T)sp.z : (T)0;
+      T r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 == (T)0) continue;
+      if (!BLOB) {
+        T kk;
+        if (r2 > under) {
+          kk = (T)1 / r2;
+        } else {
+          T rn = sqrt(r2);
+          T e = exp(-rn * inv_eps);
+          kk = ((T)1 - e) / (rn * (rn + eps * e));
+        }
+        T tz = kk * (T)w.z;
+        ax += tz * dy;
+        ay -= tz * dx;
+        az += kk * (dx * (T)w.y - dy * (T)w.x);
+      } else {
+        T s = r2 + d2;
+        T kk = (T)1 / (s * sqrt(s));
+        ax += kk * (dy * (T)w.z - dz * (T)w.y);
+        ay += kk * (dz * (T)w.x - dx * (T)w.z);
+        az += kk * (dx * (T)w.y - dy * (T)w.x);
+      }
+    }
+  }
+  if (i < 0) return;
+  const T coef = BLOB ? (T)P.blob_coef : (T)P.vvpe_coef;
+  out[(int64_t)t * 4 + 0] = ax * coef;
+  out[(int64_t)t * 4 + 1] = ay * coef;
+  out[(int64_t)t * 4 + 2] = az * coef;
+  out[(int64_t)t * 4 + 3] = 0;
+}
+
+template <int D>
+static int bs_dispatch(dv_ctx* c, const dv_fields* f, const int32_t* targets, int nt, void* out,
+                       int precision) {
+  const int nb = dv_blocks(nt, FT);
+  const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  const int32_t* ns = c->d_flag + 2;
+  if (precision == 64) {
+    if (blob)
+      k_bs_full<D, double, true><<<nb, FT, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt,
+                                                           (double*)out);
+    else
+      k_bs_full<D, double, false><<<nb, FT, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt,
+                                                            (double*)out);
+  } else {
+    if (blob)
+      k_bs_full<D, float, true><<<nb, FT, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt,
+                                                          (float*)out);
+    else
+      k_bs_full<D, float, false><<<nb, FT, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt,
+                                                           (float*)out);
+  }
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+DV_API int dv_bs_full(dv_ctx* c, const dv_fields* f, const float* omega, const int32_t* targets,
+                      int32_t nt, void* out, int32_t precision) {
+  if (!c || !f || !f->x || !f->material || !omega || !out) return DV_EINVAL;
+  if (precision != 32 && precision != 64)
+    return dv_fail(c, DV_EINVAL, "dv_bs_full: precision must be 32 or 64");
+  if (nt < 0 || nt > c->cap) return dv_fail(c, DV_EINVAL, "dv_bs_full: nt=%d out of range", nt);
+  if (nt == 0) return DV_OK;
+  const int m = (int)std::min<int64_t>(c->n_upper, c->cap) + 1;
+  const int nb = dv_blocks(m);
+  if (c->p.dim == 2)
+    k_flag_fluid<2><<<nb, DV_THREADS, 0, c->stream>>>(*f, c->d_cnt, m, c->flags);
+  else
+    k_flag_fluid<3><<<nb, DV_THREADS, 0, c->stream>>>(*f, c->d_cnt, m, c->flags);
+  DV_LAUNCHED(c);
+  int rc = dv_scan_u32(c, c->flags, c->offs, m);
+  if (rc) return rc;
+  if (c->p.dim == 2)
+    k_pack_sources<2><<<nb, DV_THREADS, 0, c->stream>>>(*f, omega, c->flags, c->offs, c->d_cnt, c->spos,
+                                                        c->sw, c->d_flag + 2);
+  else
+    k_pack_sources<3><<<nb, DV_THREADS, 0, c->stream>>>(*f, omega, c->flags, c->offs, c->d_cnt, c->spos,
+                                                        c->sw, c->d_flag + 2);
+  DV_LAUNCHED(c);
+  return c->p.dim == 2 ? bs_dispatch<2>(c, f, targets, nt, out, precision)
+                       : bs_dispatch<3>(c, f, targets, nt, out, precision);
+}

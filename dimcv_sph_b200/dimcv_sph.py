@@ -1,0 +1,282 @@
+"""SPHBase / DIMCVSPHSolver with the reference's method names
+(sph_base.py:5-232, dimcv_sph.py:6-819); every method is one or a few
+libdimcv calls on the particle system's current field set.
+
+Sampling (new options, defaults = reference):
+  samplerMode  "bernoulli" (dimcv_sph.py:305-335, Philox in place of the
+               time-seeded ti.random), "inverse_cdf" (M draws from the FP64
+               AKDE CDF) or "injected" (the caller fills sample_idx);
+  mcSamples    M for inverse_cdf as an int, or a fraction of the fluid count;
+  seed         RNG seed (default 0).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._abi import DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF
+from .particle_system import Scalar
+
+_MODES = {"bernoulli": DV_SAMPLE_BERNOULLI, "inverse_cdf": DV_SAMPLE_INVERSE_CDF,
+          "injected": DV_SAMPLE_INJECTED}
+
+
+class SPHBase:
+    def __init__(self, particle_system):
+        self.ps = particle_system
+        self.lib = self.ps.lib
+        self.ctx = self.ps.ctx
+        g = self.ps.cfg.get_cfg
+        self.g = np.array(g("gravitation"))
+        self.viscosity = 1e-3
+        self.density_0 = g("density0") if g("density0") is not None else 1000.0
+        self._dt = float(np.float32(g("timeStepSize") if g("timeStepSize") is not None else 1e-4))
+        self.dt = Scalar(lambda: self._dt, self._set_dt)
+
+    def _set_dt(self, value):
+        # the reference keeps inv_dt / inv_dt2 from construction time
+        # (dimcv_sph.py:27-28); only dt itself changes here too
+        self._dt = float(np.float32(value))
+        self.ps.params.dt = self._dt
+        _lib.check(self.ctx, self.lib.dv_set_params(self.ctx, C.byref(self.ps.params)), "dv_set_params")
+
+    def _call(self, name, *args):
+        fn = getattr(self.lib, name)
+        return _lib.check(self.ctx, fn(self.ctx, C.byref(self.ps.fields_struct), *args), name)
+
+    def _calls(self, name, *args):
+        fn = getattr(self.lib, name)
+        return _lib.check(self.ctx, fn(self.ctx, C.byref(self.ps.fields_struct),
+                                       C.byref(self.ps.solver_buf.struct), *args), name)
+
+    def initialize(self):  # sph_base.py:80-85
+        self.ps.initialize_particle_system()
+        self.compute_static_boundary_volume()
+        self.compute_moving_boundary_volume()
+
+    def compute_static_boundary_volume(self):  # sph_base.py:91-98
+        self._call("dv_boundary_volume")
+
+    def compute_moving_boundary_volume(self):
+        """sph_base.py:105-112: dynamic rigid bodies are not supported, so there
+        is nothing to update."""
+
+    def substep(self):
+        pass
+
+    def step(self):  # sph_base.py:224-232
+        self.ps.initialize_particle_system()
+        self.compute_moving_boundary_volume()
+        self.substep()
+
+
+class DIMCVSPHSolver(SPHBase):
+    def __init__(self, particle_system):
+        super().__init__(particle_system)
+        g = self.ps.cfg.get_cfg
+        self.surface_tension = 0
+        self.eps = 1e-6
+        self.inv_eps = 1.0 / self.eps
+        self.volume_scale = g("volumeScale")
+        if self.volume_scale is not None:
+            self.vp_volume = self.volume_scale * self.ps.m_V0
+        self.m_max_iterations_v = int(g("maxIterationsV") or 100)
+        self.m_max_iterations = int(g("maxIterations") or 100)
+        self.m_eps = 1e-5
+        self.max_error_V = 0.1
+        self.max_error = 0.05
+        self.inv_dt = 1.0 / self._dt
+        self.inv_dt2 = 1.0 / (self._dt * self._dt)
+        self.vortex_enforcing_domain_start = g("vortexEnforcingDomainStart")
+        self.vortex_enforcing_domain_end = g("vortexEnforcingDomainEnd")
+        self.a = g("GenProbPara")
+        self.b = g("DelProbPara")
+        self.divergence_transit_area = g("divergenceTransitArea")
+        self.sampler = g("samplerMode") or "bernoulli"
+        if self.sampler not in _MODES:
+            raise ValueError(f"samplerMode must be one of {sorted(_MODES)}")
+        self.mc_samples = g("mcSamples")
+        self.seed = int(g("seed") or 0)
+        self.rng_step = 0
+        self.injected_num_samples = 0
+        self.last_iters = (0, 0)
+        # emitter interval (dimcv_sph.py:66-74)
+        self.cnt = 0
+        self.emit_interval = 1
+        for emitter in self.ps.fluid_emitters:
+            init_v = np.array(emitter["velocity"])
+            self.emit_interval = int(np.ceil(self.ps.particle_diameter / (np.linalg.norm(init_v) * self._dt)))
+            break
+        sb = self.ps.solver_buf
+        self.num_samples = Scalar(lambda: self.ps.counters()["num_samples"], self._set_num_samples)
+        self.kden_sum = Scalar(lambda: self.ps.counters()["kden_sum_f32"])
+        self._sb = sb
+
+    # solver fields (index-stable; views of the padded buffers)
+    d_vort = property(lambda self: self._sb["d_vort"][:, :3])
+    d_vort_smoothed = property(lambda self: self._sb["d_vort_smoothed"][:, :3])
+    v_star = property(lambda self: self._sb["v_star"][:, : self.ps.dim])
+    grad_v = property(lambda self: self._sb["grad_v"].view(-1, self.ps.dim, self.ps.dim))
+    x_temp = property(lambda self: self._sb["x_temp"][:, : self.ps.dim])
+    sample_idx = property(lambda self: self._sb["sample_idx"])
+    kinematic_vort_num = property(lambda self: self._sb["kvn"])
+    kernel_density = property(lambda self: self._sb["kden"])
+    v_vort = property(lambda self: self._sb["v_vort"][:, :3])
+
+    def _set_num_samples(self, value):
+        self.injected_num_samples = int(value)
+        self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(value))
+
+    # ----------------------------------------------------------- DFSPH
+    def compute_DFSPH_factor(self):  # dimcv_sph.py:86-106
+        self._call("dv_dfsph_factor")
+
+    def compute_densities(self):  # :139-148
+        self._call("dv_densities")
+
+    def compute_non_pressure_forces(self):  # :195-208
+        self._call("dv_nonpressure")
+
+    def advect(self):  # :210-218
+        self._call("dv_advect")
+
+    def predict_velocity(self):  # :220-226
+        self._call("dv_predict_velocity")
+
+    def compute_density_change(self):  # :337-358
+        self._call("dv_density_change")
+
+    def multiply_time_step(self, field, time_step):  # :395-399
+        if field is not None and field is not self.ps.dfsph_factor and \
+                field.data_ptr() != self.ps.dfsph_factor.data_ptr():
+            raise ValueError("multiply_time_step is defined for ps.dfsph_factor only")
+        self._call("dv_scale_factor", float(np.float32(time_step)))
+
+    def compute_density_error(self, offset):  # :407-419 (FP64 sum)
+        out = C.c_double()
+        self._call("dv_density_error", float(np.float32(offset)), C.byref(out))
+        return out.value
+
+    def divergence_solver_iteration_kernel(self):  # :421-443
+        self._call("dv_divergence_iteration")
+
+    def compute_density_adv(self):  # :470-479
+        self._call("dv_density_adv")
+
+    def pressure_solve_iteration_kernel(self):  # :495-508
+        self._call("dv_pressure_iteration")
+
+    def pressure_solve_iteration(self):  # :585-589
+        self.pressure_solve_iteration_kernel()
+        self.compute_density_adv()
+        return self.compute_density_error(self.density_0) / self.ps.fluid_particle_num[None]
+
+    def divergence_solver_iteration(self):  # :591-595
+        self.divergence_solver_iteration_kernel()
+        self.compute_density_change()
+        return self.compute_density_error(0.0) / self.ps.fluid_particle_num[None]
+
+    def divergence_solve(self):
+        """dimcv_sph.py:376-393, with the Jacobi loop on the device."""
+        it = C.c_int32(0)
+        self._call("dv_divergence_solve", C.byref(it) if self.track_iterations else None)
+        self.last_iters = (it.value, self.last_iters[1])
+
+    def pressure_solve(self):
+        """dimcv_sph.py:597-614, with the Jacobi loop on the device."""
+        it = C.c_int32(0)
+        self._call("dv_pressure_solve", C.byref(it) if self.track_iterations else None)
+        self.last_iters = (self.last_iters[0], it.value)
+
+    track_iterations = False
+
+    # ----------------------------------------------------------- DIMCV
+    def compute_v_star(self):  # :264-271 (computed with vorticity and ∇v)
+        self._calls("dv_dimcv_vorticity")
+
+    def compute_vorticity(self):  # :284-293
+        self._calls("dv_dimcv_vorticity")
+
+    def compute_grad_v(self):  # :273-282
+        self._calls("dv_dimcv_vorticity")
+
+    def init(self):  # :803-806 — one fused sweep for v*, ω and ∇v
+        self._calls("dv_dimcv_vorticity")
+
+    def compute_d_vorticity(self):  # :573-583
+        self._calls("dv_d_vorticity")
+
+    def compute_all_d_vort_smoothed(self):  # :666-677
+        self._calls("dv_smooth_d_vort")
+
+    def compute_kinematic_vorticity_num_sample(self):  # :305-324
+        bd = 1 if self.sampler == "bernoulli" else 0
+        self._calls("dv_kvn_sample", self.seed, self.rng_step, bd)
+
+    def record_vort_part_sample_idx(self):  # :326-335
+        if self.sampler == "bernoulli":
+            self._calls("dv_record_samples")
+
+    def update_sample(self):  # :808-810
+        self.compute_kinematic_vorticity_num_sample()
+        self.record_vort_part_sample_idx()
+
+    def compute_kernel_density(self):  # :738-751
+        self._calls("dv_akde")
+
+    def _draw_samples(self):
+        if self.sampler == "inverse_cdf":
+            M = self.mc_samples
+            if M is None:
+                M = 1.0 / 16.0
+            if isinstance(M, float) and M <= 1.0:
+                M = max(1, int(M * self.ps.fluid_particle_num[None]))
+            self._calls("dv_sample", DV_SAMPLE_INVERSE_CDF, self.seed, self.rng_step, int(M))
+        elif self.sampler == "injected":
+            self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(self.injected_num_samples))
+
+    def vort2vel(self):  # :679-719
+        self._calls("dv_vvpe_mc")
+
+    def update_particle_life_time(self):  # :753-760
+        self._call("dv_life_time")
+
+    def copy_x_temp(self):  # :797-801 (with compute_vorticity_vis)
+        self._calls("dv_vis")
+
+    def compute_vorticity_vis(self):  # :785-795 — done by copy_x_temp's fused sweep
+        pass
+
+    def dimcv(self):  # :812-819
+        self.init()
+        self.compute_d_vorticity()
+        self.compute_all_d_vort_smoothed()
+        self.update_sample()
+        self.compute_kernel_density()
+        self._draw_samples()
+        self.vort2vel()
+        self.update_particle_life_time()
+        self.rng_step += 1
+
+    # ----------------------------------------------------------- emission
+    def emit_particle(self):  # :616-637
+        for emitter in self.ps.fluid_emitters:
+            obj_id = emitter["objectId"]
+            center = np.array(emitter["squareCenter"])
+            size = np.array(emitter["squareSize"])
+            init_v = np.array(emitter["velocity"])
+            lower = center - 0.5 * size
+            cube = size + self.ps.particle_radius * np.abs(init_v) / np.linalg.norm(init_v)
+            self.ps.object_collection[obj_id]["particleNum"] += self.ps.compute_cube_particle_num(lower, lower + cube)
+            self.ps.add_cube(object_id=obj_id, lower_corner=lower, cube_size=cube, velocity=init_v,
+                             density=emitter["density"], is_dynamic=1, color=emitter["color"], material=1)
+
+    def dump_num_particles_each_emitters_ti2np(self):  # :639-642
+        """Emitter bookkeeping is computed on demand (ps.num_particles_each_emitter)
+        instead of a device read every step."""
+
+    def dump_num_particles_each_emitters_np2ti(self):  # :644-647
+        """See dump_num_particles_each_emitters_ti2np."""

@@ -1,0 +1,67 @@
+"""Host-side parameter derivation and scene builders (no GPU)."""
+import numpy as np
+import pytest
+
+from dimcv_sph_b200 import scenes
+from dimcv_sph_b200.params import f32_pow_int, make_params, sqrt_limits
+
+
+@pytest.mark.parametrize("h", [0.04, 0.016, 0.018, 0.0390625, 1e-3, 3.3e-2])
+def test_sqrt_limits_are_exact(h):
+    lo, hi = sqrt_limits(h)
+    h32 = np.float32(h)
+    lo32, hi32 = np.float32(lo), np.float32(hi)
+    assert np.sqrt(lo32) >= h32 and np.sqrt(np.nextafter(lo32, np.float32(0))) < h32
+    assert np.sqrt(hi32) <= h32 and np.sqrt(np.nextafter(hi32, np.float32(np.inf))) > h32
+    # exhaustive check on the f32 values around h^2
+    t = np.float32(h32 * h32)
+    for k in range(-64, 65):
+        v = t
+        step = np.float32(np.inf) if k > 0 else np.float32(0)
+        for _ in range(abs(k)):
+            v = np.nextafter(v, step)
+        assert (np.sqrt(v) < h32) == (v < lo32)
+        assert (np.sqrt(v) > h32) == (v > hi32)
+
+
+def test_pow_by_squaring():
+    h = np.float32(25.0)
+    assert f32_pow_int(h, 2) == np.float32(h * h)
+    assert f32_pow_int(h, 3) == np.float32(np.float32(h * h) * h)
+
+
+def test_channel_params_follow_reference_expressions():
+    cfg = scenes.channel2d()
+    p = make_params(cfg)
+    assert p.dim == 2 and list(p.grid_num)[:2] == [100, 25]
+    assert p.support_radius == np.float32(0.04)
+    assert p.kW == np.float32(np.float32(1.8189) * np.float32(np.float32(25.0) * np.float32(25.0)))
+    assert p.kW2 == np.float32(2) * np.float32(p.kW)
+    assert p.neighbor_min == 7
+    dt = float(np.float32(4e-4))
+    assert p.inv_dt == np.float32(1.0 / dt)
+    assert abs(p.eta_div - (1.0 / dt) * 0.1 * 0.01 * 1000) < 1e-9
+    assert p.eta_p == 0.05 * 0.01 * 1000
+    assert p.visc_coef == np.float32(np.float32(8) * np.float32(1e-3))
+    assert p.has_transit == 1 and p.transit_span == np.float32(0.02)
+    assert p.skip_cell0 == 1 and p.kernel_mode == 0
+
+
+def test_sphere_grid_matches_config():
+    cfg = scenes.sphere3d()
+    p = make_params(cfg)
+    assert list(p.grid_num) == [188, 63, 63]
+    assert p.neighbor_min == 20
+
+
+def test_ring_scene_volume_and_offset():
+    cfg, x, w = scenes.ring3d(4096, seed=1)
+    p = make_params(cfg)
+    assert p.cell_origin_offset == 1 and p.skip_cell0 == 0 and p.kernel_mode == 1
+    assert x.shape == (4096, 3) and np.all(np.abs(x) <= 1.0)
+    r = 0.5 * (8.0 / 4096) ** (1 / 3)
+    vp = 1.25 * 0.8 * (2 * r) ** 3
+    assert abs(vp - 8.0 / 4096) < 1e-12
+    # the ring peak vorticity is Γ/(πσ²) on the core circle
+    c = np.array([[0.5, 0.0, 0.0]])
+    assert abs(np.linalg.norm(scenes.ring_vorticity(c)) - 1.0 / (np.pi * 0.05 ** 2)) < 1e-9
