@@ -62,6 +62,7 @@ PROTOTYPES = {
     "dv_vis": (C.c_int, [_P, _FP, _SP]),
     "dv_bs_full": (C.c_int, [_P, _FP, _P, _P, i32, _P, i32]),
     "dv_fp32_peak": (C.c_int, [_P, C.POINTER(f64)]),
+    "dv_density_error_noalloc": (C.c_int, [_PP, _FP, i32, f32, C.POINTER(f64), _P]),
     "dv_profile": (C.c_int, [_P, i32]),
     "dv_profile_read": (C.c_int, [_P, C.POINTER(f64), C.POINTER(i64), C.POINTER(f64)]),
 }

@@ -30,6 +30,7 @@ UNITS = {
     "dv_sph.cu": ["-fmad=false"],
     "dv_dimcv.cu": ["-fmad=false"],
     "dv_vvpe.cu": [],
+    "dv_noalloc.cu": ["-fmad=false"],
 }
 
 
