@@ -58,6 +58,8 @@ PROTOTYPES = {
     "dv_akde": (C.c_int, [_P, _FP, _SP]),
     "dv_sample": (C.c_int, [_P, _FP, _SP, i32, u64, u64, i32]),
     "dv_vvpe_mc": (C.c_int, [_P, _FP, _SP]),
+    "dv_autotune": (C.c_int, [_P, _FP, _SP, C.POINTER(i32), C.POINTER(f32)]),
+    "dv_set_far_tile": (C.c_int, [_P, i32]),
     "dv_life_time": (C.c_int, [_P, _FP]),
     "dv_vis": (C.c_int, [_P, _FP, _SP]),
     "dv_bs_full": (C.c_int, [_P, _FP, _P, _P, i32, _P, i32]),

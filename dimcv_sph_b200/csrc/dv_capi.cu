@@ -103,7 +103,8 @@ DV_API void dv_destroy(dv_ctx* c) {
   void* ptrs[] = {c->d_cnt,   c->d_flag,    c->keys[0],   c->keys[1],   c->vals[0], c->vals[1],
                   c->hist,    c->cell_start, c->cell_end, c->mt[0],     c->mt[1],   c->mt[2],
                   c->scan_part, c->dscan_part, c->red_part, c->ired_part, c->flags, c->offs,
-                  c->targets, c->cdf,       c->spos,      c->sw,        c->near_v,  c->near_S};
+                  c->targets, c->cdf,       c->spos,      c->sw,        c->near_v,  c->near_S,
+                  c->far_acc, c->mult};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2 * dv_ctx::kProfPool; ++k)
@@ -167,6 +168,8 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   A(c->sw, cap);
   A(c->near_v, cap);
   A(c->near_S, cap);
+  A(c->far_acc, cap);
+  A(c->mult, cap);
   A(c->d_prof, 4);
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_cnt, sizeof(dv_counters));

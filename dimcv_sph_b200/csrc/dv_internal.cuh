@@ -63,6 +63,9 @@ struct dv_ctx {
   float4* sw = nullptr;        // cap
   float4* near_v = nullptr;    // cap
   float* near_S = nullptr;     // cap
+  float4* far_acc = nullptr;   // cap: far-field sums of the main loop, per target
+  int32_t* mult = nullptr;     // cap: sample multiplicity per slot
+  int far_tt = 4;              // targets per thread of the far-field main loop (autotuned)
 
   // far-field kernel profiling (dv_profile)
   bool prof = false;

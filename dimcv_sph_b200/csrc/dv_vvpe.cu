@@ -206,6 +206,270 @@ static bool fast_kernel_ok(const dv_params& P) {
   return (double)P.support_radius * (double)P.inv_eps > 104.5;
 }
 
+// ------------------------------------------------- far field, split form
+// The main loop evaluates every (target, sample) pair WITHOUT the far test:
+// for the reference kernel the weight is 1/max(|r|², T) with T =
+// far_r2_limit, so a near sample (|r| <= h, including the target itself)
+// adds a bounded term (|r_xy|/T·|ω̂| <= |ω̂|/h, the size of the largest far
+// terms).  A second kernel then finds, per target, the few samples with
+// |r| <= h — exactly, with the reference's non-FMA |r|² test — among the
+// particles of the target's cell window, subtracts their terms (recomputed
+// bit for bit as the main loop computed them) and removes them from the far
+// count.  Per pair this leaves ~14 issue slots instead of ~28.
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// one pair of the main loop: returns the three increments (r × ω̂ weighted)
+template <int D, bool BLOB>
+__device__ __forceinline__ void far_terms(float px, float py, float pz, float4 sp, float4 w, float lim,
+                                          float d2, float& cx, float& cy, float& cz) {
+  const float dx = __fsub_rn(px, sp.x);
+  const float dy = __fsub_rn(py, sp.y);
+  const float dz = D == 3 ? __fsub_rn(pz, sp.z) : 0.0f;
+  float r2 = __fmul_rn(dx, dx);
+  r2 = __fmaf_rn(dy, dy, r2);
+  if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
+  if (!BLOB) {
+    // Kε = 1/|r|² (exp term underflows for |r| > h); cross with r_xy = (dx, dy, 0)
+    const float kk = rcp_approx(fmaxf(r2, lim));
+    const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy);
+    cx = __fmul_rn(b, w.z);
+    cy = -__fmul_rn(a, w.z);
+    cz = __fmaf_rn(a, w.y, -__fmul_rn(b, w.x));
+  } else {
+    const float inv = rsqrtf(__fadd_rn(r2, d2));
+    const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
+    const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
+    cx = __fmaf_rn(b, w.z, -__fmul_rn(e, w.y));
+    cy = __fmaf_rn(e, w.x, -__fmul_rn(a, w.z));
+    cz = __fmaf_rn(a, w.y, -__fmul_rn(b, w.x));
+  }
+}
+
+// main loop accumulation form of far_terms (lets the increments fuse into FMAs)
+template <int D, bool BLOB, bool COMP>
+__device__ __forceinline__ void far_accum(float px, float py, float pz, float4 sp, float4 w, float lim, float d2,
+                                          Acc<COMP>& ax, Acc<COMP>& ay, Acc<COMP>& az) {
+  const float dx = __fsub_rn(px, sp.x);
+  const float dy = __fsub_rn(py, sp.y);
+  const float dz = D == 3 ? __fsub_rn(pz, sp.z) : 0.0f;
+  float r2 = __fmul_rn(dx, dx);
+  r2 = __fmaf_rn(dy, dy, r2);
+  if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
+  if (COMP) {
+    float cx, cy, cz;
+    far_terms<D, BLOB>(px, py, pz, sp, w, lim, d2, cx, cy, cz);
+    ax.add(cx);
+    ay.add(cy);
+    az.add(cz);
+  } else if (!BLOB) {
+    const float kk = rcp_approx(fmaxf(r2, lim));
+    const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy);
+    ax.s = __fmaf_rn(b, w.z, ax.s);
+    ay.s = __fmaf_rn(-a, w.z, ay.s);
+    az.s = __fmaf_rn(a, w.y, az.s);
+    az.s = __fmaf_rn(-b, w.x, az.s);
+  } else {
+    const float inv = rsqrtf(__fadd_rn(r2, d2));
+    const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
+    const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
+    ax.s = __fmaf_rn(b, w.z, ax.s);
+    ax.s = __fmaf_rn(-e, w.y, ax.s);
+    ay.s = __fmaf_rn(e, w.x, ay.s);
+    ay.s = __fmaf_rn(-a, w.z, ay.s);
+    az.s = __fmaf_rn(a, w.y, az.s);
+    az.s = __fmaf_rn(-b, w.x, az.s);
+  }
+}
+
+#define FT2 256
+#define FTILE2 512
+
+template <int D, int TT, bool BLOB, bool COMP>
+__global__ void __launch_bounds__(FT2) k_far_main(dv_params P, const float* __restrict__ x,
+                                                  const dv_counters* __restrict__ C,
+                                                  const int32_t* __restrict__ targets,
+                                                  const float4* __restrict__ spos,
+                                                  const float4* __restrict__ sw,
+                                                  float4* __restrict__ far_acc) {
+  __shared__ float4 s_p[FTILE2];
+  __shared__ float4 s_w[FTILE2];
+  const int nt = C->n_targets;
+  const int M = C->num_samples;
+  const int tbase = blockIdx.x * FT2 * TT;
+  if (tbase >= nt) return;  // uniform per CTA
+  float px[TT], py[TT], pz[TT];
+  Acc<COMP> ax[TT], ay[TT], az[TT];
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT2 + threadIdx.x;
+    V3 xi = ldv<D>(x, targets[t < nt ? t : nt - 1]);
+    px[k] = xi.x;
+    py[k] = xi.y;
+    pz[k] = xi.z;
+  }
+  const float lim = P.far_r2_limit;
+  const float d2 = P.blob_delta2;
+  for (int base = 0; base < M; base += FTILE2) {
+    const int m = min(FTILE2, M - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT2) {
+      s_p[q] = spos[base + q];
+      s_w[q] = sw[base + q];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < m; ++q) {
+      const float4 sp = s_p[q];
+      const float4 w = s_w[q];
+#pragma unroll
+      for (int k = 0; k < TT; ++k) far_accum<D, BLOB, COMP>(px[k], py[k], pz[k], sp, w, lim, d2, ax[k], ay[k], az[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT2 + threadIdx.x;
+    if (t < nt) far_acc[t] = make_float4(ax[k].val(), ay[k].val(), az[k].val(), 0.0f);
+  }
+}
+
+// sample multiplicities per slot (a slot may be drawn several times)
+__global__ void k_mult(const int32_t* __restrict__ sample_idx, const dv_counters* __restrict__ C,
+                       int32_t* __restrict__ mult) {
+  const int M = C->num_samples, n = C->n;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < M; s += gridDim.x * blockDim.x) {
+    int j = sample_idx[s];
+    if (j >= 0 && j < n) atomicAdd(mult + j, 1);
+  }
+}
+
+// cell window of a target that contains every particle within h: the 3^d
+// cells around its cell, widened by one cell on a side where the target's
+// cell coordinate is within rounding of a cell face (a particle exactly h
+// away can then sit two cells over)
+__device__ __forceinline__ void far_window(const dv_params& P, float xv, int d, int& lo, int& hi) {
+  float t = P.cell_origin_offset ? (xv - P.domain_start[d]) : xv;
+  float q = t / P.grid_size;
+  int c = cell_coord(P, xv, d);
+  float tol = 4.8e-7f * fmaxf(1.0f, fabsf(q));
+  float frac = q - (float)c;
+  lo = c - 1 - (frac <= tol ? 1 : 0);
+  hi = c + 1 + (frac >= 1.0f - tol ? 1 : 0);
+  lo = max(lo, 0);
+  hi = min(hi, P.grid_num[d] - 1);
+}
+
+template <int D, bool BLOB>
+__global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                          const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
+                          const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
+                          const float4* __restrict__ near_v, const float* __restrict__ near_S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nt = C->n_targets;
+  if (t >= nt) return;
+  const int M = C->num_samples;
+  const int i = targets[t];
+  const V3 xi = ldv<D>(F.x, i);
+  const float lim = P.far_r2_limit, d2 = P.blob_delta2;
+  float4 acc = far_acc[t];
+  int near_cnt = 0;
+  int lo0, hi0, lo1, hi1, lo2 = 0, hi2 = 0;
+  far_window(P, xi.x, 0, lo0, hi0);
+  far_window(P, xi.y, 1, lo1, hi1);
+  if (D == 3) far_window(P, xi.z, 2, lo2, hi2);
+  for (int a = lo0; a <= hi0; ++a) {
+    const uint32_t ka = __ldg(G.mt0 + a);
+    for (int b = lo1; b <= hi1; ++b) {
+      const uint32_t kab = ka | __ldg(G.mt1 + b);
+      for (int cc = lo2; cc <= hi2; ++cc) {
+        const uint32_t key = D == 3 ? (kab | __ldg(G.mt2 + cc)) : kab;
+        const int s0 = __ldg(G.start + key), e0 = __ldg(G.end + key);
+        for (int j = s0; j < e0; ++j) {
+          const int m = mult[j];
+          if (m == 0) continue;
+          const V3 xj = ldv<D>(F.x, j);
+          V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
+          if (sqnorm<D>(r) > lim) continue;  // far: the main loop's term stays
+          near_cnt += m;
+          const V3 w3 = ld4(S.d_vort_smoothed, j);
+          const float inv = 1.0f / (S.kden[j] + P.kden_eps);
+          const float4 w = make_float4(w3.x * inv, w3.y * inv, w3.z * inv, 0.0f);
+          float cx, cy, cz;
+          far_terms<D, BLOB>(xi.x, xi.y, xi.z, make_float4(xj.x, xj.y, xj.z, 0.0f), w, lim, d2, cx, cy, cz);
+          const float fm = (float)m;
+          acc.x = __fmaf_rn(-fm, cx, acc.x);
+          acc.y = __fmaf_rn(-fm, cy, acc.y);
+          acc.z = __fmaf_rn(-fm, cz, acc.z);
+        }
+      }
+    }
+  }
+  const int cnt = M - near_cnt;
+  const float coef = BLOB ? P.blob_coef : P.vvpe_coef;
+  const float fac = C->kden_sum_f32 - near_S[t];
+  V3 fv{0.f, 0.f, 0.f};
+  if (cnt > 0) {
+    const float sc = coef / (float)cnt;
+    fv.x = (acc.x * fac) * sc;
+    fv.y = (acc.y * fac) * sc;
+    fv.z = (acc.z * fac) * sc;
+  }
+  const float4 nv = near_v[t];
+  V3 vv{__fadd_rn(fv.x, nv.x), __fadd_rn(fv.y, nv.y), __fadd_rn(fv.z, nv.z)};
+  if (S.v_vort) st4(S.v_vort, i, vv);
+  // gate ‖v_vort‖ < ‖v_i‖ (dimcv_sph.py:717-719)
+  const float n1 = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vv.x, vv.x), __fmul_rn(vv.y, vv.y)), __fmul_rn(vv.z, vv.z)));
+  V3 v = ldv<D>(F.v, i);
+  const float n2 = sqrtf(sqnorm<D>(v));
+  if (n1 < n2) {
+    v.x = __fadd_rn(v.x, vv.x);
+    v.y = __fadd_rn(v.y, vv.y);
+    if (D == 3) v.z = __fadd_rn(v.z, vv.z);
+    stv<D>(F.v, i, v);
+  }
+}
+
+template <int D, bool BLOB, bool COMP>
+static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
+  const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
+  const int nb = (int)std::max<int64_t>(1, (nu + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
+#define L(TTV)                                                                                          \
+  k_far_main<D, TTV, BLOB, COMP><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
+                                                            c->sw, c->far_acc)
+  if (tt <= 2)
+    L(2);
+  else if (tt <= 4)
+    L(4);
+  else
+    L(8);
+#undef L
+}
+
+template <int D>
+static void launch_main(dv_ctx* c, const dv_fields* f, int tt) {
+  const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  const bool comp = c->p.compensated != 0;
+  if (blob)
+    comp ? launch_main_tt<D, true, true>(c, f, tt) : launch_main_tt<D, true, false>(c, f, tt);
+  else
+    comp ? launch_main_tt<D, false, true>(c, f, tt) : launch_main_tt<D, false, false>(c, f, tt);
+}
+
+template <int D>
+static void launch_fix(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
+  const int nb = dv_blocks(std::min<int64_t>(c->n_upper, c->cap), 128);
+  if (c->p.kernel_mode == DV_KERNEL_BLOB3D)
+    k_far_fix<D, true><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,
+                                                  c->far_acc, c->near_v, c->near_S);
+  else
+    k_far_fix<D, false><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,
+                                                   c->far_acc, c->near_v, c->near_S);
+}
+
 __global__ void k_prof_pairs(const dv_counters* __restrict__ C, double* acc) {
   acc[0] += (double)C->n_targets * (double)C->num_samples;
 }
@@ -247,6 +511,59 @@ DV_API int dv_profile_read(dv_ctx* c, double* far_ms, int64_t* launches, double*
   return DV_OK;
 }
 
+// Times the far-field main loop for 2, 4 and 8 targets per thread on the
+// current targets and samples (CUDA events, best of two launches after one
+// warm-up) and keeps the fastest for this context.
+DV_API int dv_autotune(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, int32_t* best_tt,
+                       float* best_ms) {
+  if (!c || !f || !s || !s->sample_idx) return DV_EINVAL;
+  if (!fast_kernel_ok(c->p) && c->p.kernel_mode != DV_KERNEL_BLOB3D) return DV_OK;
+  int rc = dv_build_targets(c, f);
+  if (rc) return rc;
+  const int packb = c->num_sms * 4;
+  if (c->p.dim == 2)
+    k_pack_samples<2><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw, c->p.kden_eps);
+  else
+    k_pack_samples<3><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw, c->p.kden_eps);
+  DV_LAUNCHED(c);
+  cudaEvent_t e0, e1;
+  DV_CK(c, cudaEventCreate(&e0));
+  DV_CK(c, cudaEventCreate(&e1));
+  const int cand[3] = {2, 4, 8};
+  float best = 1e30f;
+  int best_t = c->far_tt;
+  for (int tt : cand) {
+    for (int rep = 0; rep < 3; ++rep) {
+      DV_CK(c, cudaEventRecord(e0, c->stream));
+      if (c->p.dim == 2)
+        launch_main<2>(c, f, tt);
+      else
+        launch_main<3>(c, f, tt);
+      DV_LAUNCHED(c);
+      DV_CK(c, cudaEventRecord(e1, c->stream));
+      DV_CK(c, cudaEventSynchronize(e1));
+      float ms = 0.f;
+      DV_CK(c, cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0 && ms < best) {
+        best = ms;
+        best_t = tt;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->far_tt = best_t;
+  if (best_tt) *best_tt = best_t;
+  if (best_ms) *best_ms = best;
+  return DV_OK;
+}
+
+DV_API int dv_set_far_tile(dv_ctx* c, int32_t tt) {
+  if (!c || (tt != 2 && tt != 4 && tt != 8)) return DV_EINVAL;
+  c->far_tt = tt;
+  return DV_OK;
+}
+
 DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   if (!c || !f || !s || !s->sample_idx || !s->kden || !s->d_vort_smoothed)
     return c ? dv_fail(c, DV_EINVAL, "dv_vvpe_mc: NULL field") : DV_EINVAL;
@@ -263,8 +580,12 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
                                                           c->p.kden_eps);
   DV_LAUNCHED(c);
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
-  const int nb = (int)std::max<int64_t>(1, (nu + FT * 2 - 1) / (FT * 2));
-  const bool fastk = fast_kernel_ok(c->p);
+  const bool fastk = fast_kernel_ok(c->p) || c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  if (fastk) {  // split form: sample multiplicities for the correction kernel
+    DV_CK(c, cudaMemsetAsync(c->mult, 0, sizeof(int32_t) * nu, c->stream));
+    k_mult<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(s->sample_idx, c->d_cnt, c->mult);
+    DV_LAUNCHED(c);
+  }
   if (c->prof) {
     if (c->prof_used == dv_ctx::kProfPool) {
       int rc2 = prof_fold(c);
@@ -272,13 +593,30 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
     }
     DV_CK(c, cudaEventRecord(c->prof_ev[2 * c->prof_used], c->stream));
   }
-  if (c->p.dim == 2)
-    dispatch_far<2>(c, f, s, nb, fastk);
-  else
-    dispatch_far<3>(c, f, s, nb, fastk);
+  if (fastk) {
+    if (c->p.dim == 2)
+      launch_main<2>(c, f, c->far_tt);
+    else
+      launch_main<3>(c, f, c->far_tt);
+  } else {  // |r| > h may not underflow exp(-|r|/ε): per-pair exact kernel
+    const int nb = (int)std::max<int64_t>(1, (nu + FT * 2 - 1) / (FT * 2));
+    if (c->p.dim == 2)
+      dispatch_far<2>(c, f, s, nb, false);
+    else
+      dispatch_far<3>(c, f, s, nb, false);
+  }
   DV_LAUNCHED(c);
   if (c->prof) {
     DV_CK(c, cudaEventRecord(c->prof_ev[2 * c->prof_used + 1], c->stream));
+  }
+  if (fastk) {
+    if (c->p.dim == 2)
+      launch_fix<2>(c, f, s);
+    else
+      launch_fix<3>(c, f, s);
+    DV_LAUNCHED(c);
+  }
+  if (c->prof) {
     c->prof_used++;
     c->prof_launches++;
     k_prof_pairs<<<1, 1, 0, c->stream>>>(c->d_cnt, c->d_prof);

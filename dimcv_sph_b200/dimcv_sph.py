@@ -238,7 +238,23 @@ class DIMCVSPHSolver(SPHBase):
         elif self.sampler == "injected":
             self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(self.injected_num_samples))
 
+    autotune = True
+    far_tile = None
+
     def vort2vel(self):  # :679-719
+        if self.far_tile is None:
+            import os
+            forced = os.environ.get("DIMCV_FAR_TT")
+            if forced:
+                self.far_tile = int(forced)
+                _lib.check(self.ctx, self.lib.dv_set_far_tile(self.ctx, self.far_tile), "dv_set_far_tile")
+            elif self.autotune:
+                # one-time choice of the far-field tile (targets per thread) on this state
+                tt, ms = C.c_int32(0), C.c_float(0)
+                self._calls("dv_autotune", C.byref(tt), C.byref(ms))
+                self.far_tile = tt.value or 4
+            else:
+                self.far_tile = 4
         self._calls("dv_vvpe_mc")
 
     def update_particle_life_time(self):  # :753-760
