@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--workload", choices=["sphere3d", "channel2d"], default="sphere3d")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-vs-bs", action="store_true",
+                    help="skip the MC-VVPE vs full Biot-Savart study on the 1M-particle vortex ring")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--scale", type=float, default=1.0, help="particle radius multiplier (1 = benchmark size)")
     return ap.parse_args()
@@ -286,6 +288,11 @@ def run_ours(args, rank, world, local):
         result["e2e"] = e2e(args, ps, solver, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args, ps, solver)
+    if rank == 0 and world == 1 and not args.no_vs_bs:
+        del ps, solver
+        torch.cuda.empty_cache()
+        from dimcv_sph_b200 import ring_study
+        result["vs_full_bs"] = ring_study.run(n=1 << 20)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -24,6 +24,7 @@ DV_WARN_BAD_INDEX = 1 << 5
 DV_SAMPLE_BERNOULLI = 0
 DV_SAMPLE_INVERSE_CDF = 1
 DV_SAMPLE_INJECTED = 2
+DV_SAMPLE_STRATIFIED = 3
 
 DV_KERNEL_REF2D = 0
 DV_KERNEL_BLOB3D = 1

@@ -263,11 +263,13 @@ __global__ void k_cdf_weights(const int32_t* __restrict__ targets, const float* 
   w[k] = k < C->n_targets ? (double)kden[targets[k]] : 0.0;
 }
 
-// draw s: u ~ U[0,1) (53 bits, Philox keyed by (s, 2, step, seed)); the
-// target k with cdf_ex[k] <= u·total < cdf_ex[k] + w_k (w_k > 0)
+// draw s: u ~ U[0,1) (53 bits, Philox keyed by (s, 2, step, seed)), or in
+// stratified mode u = (s + ξ)/M with ξ that draw; the target k with
+// cdf_ex[k] <= u·total < cdf_ex[k] + w_k (w_k > 0)
 __global__ void k_cdf_draw(const double* __restrict__ cdf_ex, const int32_t* __restrict__ targets,
                            const float* __restrict__ kden, dv_counters* C, int M, uint32_t s0,
-                           uint32_t s1, uint32_t t0, uint32_t t1, int32_t* __restrict__ out) {
+                           uint32_t s1, uint32_t t0, uint32_t t1, int stratified,
+                           int32_t* __restrict__ out) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int nt = C->n_targets;
   if (nt <= 0) {
@@ -282,7 +284,9 @@ __global__ void k_cdf_draw(const double* __restrict__ cdf_ex, const int32_t* __r
   if (s == 0) C->num_samples = M;
   if (s >= M) return;
   DvRand4 rnd = dv_philox((uint32_t)s, 2u, t0, t1, s0, s1);
-  double y = dv_u01d(rnd.v[0], rnd.v[1]) * total;
+  double u = dv_u01d(rnd.v[0], rnd.v[1]);
+  if (stratified) u = ((double)s + u) / (double)M;
+  double y = u * total;
   // upper_bound(cdf_ex, y) - 1
   int lo = 0, hi = nt;
   while (lo < hi) {
@@ -478,7 +482,7 @@ DV_API int dv_sample(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, i
     k_set_num_samples<<<1, 1, 0, c->stream>>>(c->d_cnt, M);
     DV_LAUNCHED(c);
     return DV_OK;
-  } else if (mode != DV_SAMPLE_INVERSE_CDF) {
+  } else if (mode != DV_SAMPLE_INVERSE_CDF && mode != DV_SAMPLE_STRATIFIED) {
     return dv_fail(c, DV_EINVAL, "dv_sample: unknown mode %d", mode);
   }
   int rc = dv_build_targets(c, f);
@@ -492,7 +496,7 @@ DV_API int dv_sample(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, i
   if (rc) return rc;
   k_cdf_draw<<<dv_blocks(std::max(M, 1)), DV_THREADS, 0, c->stream>>>(
       c->cdf, c->targets, s->kden, c->d_cnt, M, (uint32_t)seed, (uint32_t)(seed >> 32),
-      (uint32_t)step, (uint32_t)(step >> 32), s->sample_idx);
+      (uint32_t)step, (uint32_t)(step >> 32), mode == DV_SAMPLE_STRATIFIED ? 1 : 0, s->sample_idx);
   DV_LAUNCHED(c);
   return DV_OK;
 }

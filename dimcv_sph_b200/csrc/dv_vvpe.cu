@@ -731,12 +731,86 @@ __global__ void __launch_bounds__(FT) k_bs_full(dv_params P, const float* __rest
   out[(int64_t)t * 4 + 3] = 0;
 }
 
+// FP32 full Biot-Savart with the blob kernel, in the register-tiled form of
+// the far-field main loop: the blob kernel is regular at r = 0 and the self
+// pair contributes r × ω = 0 exactly, so every (target, source) pair is
+// summed without a test.
+template <int D, int TT, bool COMP>
+__global__ void __launch_bounds__(FT2) k_bs_fast(dv_params P, const float* __restrict__ x,
+                                                 const int32_t* __restrict__ tlist, int nt,
+                                                 const float4* __restrict__ spos, const float4* __restrict__ sw,
+                                                 const int32_t* __restrict__ ns_p,
+                                                 const dv_counters* __restrict__ C, float* __restrict__ out) {
+  __shared__ float4 s_p[FTILE2];
+  __shared__ float4 s_w[FTILE2];
+  const int ns = *ns_p;
+  const int n = C->n;
+  const int tbase = blockIdx.x * FT2 * TT;
+  if (tbase >= nt) return;
+  float px[TT], py[TT], pz[TT];
+  Acc<COMP> ax[TT], ay[TT], az[TT];
+  bool ok[TT];
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT2 + threadIdx.x;
+    int i = t < nt ? (tlist ? tlist[t] : t) : 0;
+    ok[k] = t < nt && i >= 0 && i < n;
+    V3 xi = ldv<D>(x, ok[k] ? i : 0);
+    px[k] = xi.x;
+    py[k] = xi.y;
+    pz[k] = xi.z;
+  }
+  const float d2 = P.blob_delta2;
+  for (int base = 0; base < ns; base += FTILE2) {
+    const int m = min(FTILE2, ns - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT2) {
+      s_p[q] = spos[base + q];
+      s_w[q] = sw[base + q];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < m; ++q) {
+      const float4 sp = s_p[q];
+      const float4 w = s_w[q];
+#pragma unroll
+      for (int k = 0; k < TT; ++k) far_accum<D, true, COMP>(px[k], py[k], pz[k], sp, w, 0.0f, d2, ax[k], ay[k], az[k]);
+    }
+  }
+  const float coef = P.blob_coef;
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    int t = tbase + k * FT2 + threadIdx.x;
+    if (t >= nt) continue;
+    float4 o = ok[k] ? make_float4(ax[k].val() * coef, ay[k].val() * coef, az[k].val() * coef, 0.0f)
+                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    reinterpret_cast<float4*>(out)[t] = o;
+  }
+}
+
 template <int D>
 static int bs_dispatch(dv_ctx* c, const dv_fields* f, const int32_t* targets, int nt, void* out,
                        int precision) {
   const int nb = dv_blocks(nt, FT);
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   const int32_t* ns = c->d_flag + 2;
+  if (precision == 32 && blob) {
+    const int tt = c->far_tt <= 2 ? 2 : (c->far_tt <= 4 ? 4 : 8);
+    const int nbf = (int)std::max<int64_t>(1, ((int64_t)nt + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
+#define LBS(TTV, CV)                                                                                          \
+  k_bs_fast<D, TTV, CV><<<nbf, FT2, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt, \
+                                                    (float*)out)
+    const bool comp = c->p.compensated != 0;
+    if (tt == 2)
+      comp ? LBS(2, true) : LBS(2, false);
+    else if (tt == 4)
+      comp ? LBS(4, true) : LBS(4, false);
+    else
+      comp ? LBS(8, true) : LBS(8, false);
+#undef LBS
+    DV_LAUNCHED(c);
+    return DV_OK;
+  }
   if (precision == 64) {
     if (blob)
       k_bs_full<D, double, true><<<nb, FT, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt,

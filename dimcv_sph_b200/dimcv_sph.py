@@ -17,11 +17,11 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF
+from ._abi import DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED
 from .particle_system import Scalar
 
 _MODES = {"bernoulli": DV_SAMPLE_BERNOULLI, "inverse_cdf": DV_SAMPLE_INVERSE_CDF,
-          "injected": DV_SAMPLE_INJECTED}
+          "injected": DV_SAMPLE_INJECTED, "stratified": DV_SAMPLE_STRATIFIED}
 
 
 class SPHBase:
@@ -228,13 +228,13 @@ class DIMCVSPHSolver(SPHBase):
         self._calls("dv_akde")
 
     def _draw_samples(self):
-        if self.sampler == "inverse_cdf":
+        if self.sampler in ("inverse_cdf", "stratified"):
             M = self.mc_samples
             if M is None:
                 M = 1.0 / 16.0
             if isinstance(M, float) and M <= 1.0:
                 M = max(1, int(M * self.ps.fluid_particle_num[None]))
-            self._calls("dv_sample", DV_SAMPLE_INVERSE_CDF, self.seed, self.rng_step, int(M))
+            self._calls("dv_sample", _MODES[self.sampler], self.seed, self.rng_step, int(M))
         elif self.sampler == "injected":
             self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(self.injected_num_samples))
 

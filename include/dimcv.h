@@ -70,6 +70,7 @@ enum dv_status {
 #define DV_SAMPLE_BERNOULLI 0 /* reference KVN birth/death + compaction */
 #define DV_SAMPLE_INVERSE_CDF 1 /* M i.i.d. draws from p ∝ kden (FP64 CDF) */
 #define DV_SAMPLE_INJECTED 2    /* caller supplies sample_idx / num_samples */
+#define DV_SAMPLE_STRATIFIED 3  /* M stratified draws u_s = (s + ξ_s)/M through the same CDF */
 
 /* Velocity kernels for the VVPE / Biot-Savart sums. */
 #define DV_KERNEL_REF2D 0 /* reference: 0.1592 V Kε(|r|) (r_xy × ω), dimcv_sph.py:649-719 */

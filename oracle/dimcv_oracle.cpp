@@ -1034,7 +1034,9 @@ DVO_API int dvo_sample(void* h, dv_fields* f, dv_solver_fields* s, int mode, uin
     uint32_t o[4];
     philox((uint32_t)q, 2u, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
     uint64_t mant = ((uint64_t)(o[0] >> 5) << 26) | (uint64_t)(o[1] >> 6);
-    double y = (double)mant * (1.0 / 9007199254740992.0) * run;
+    double u = (double)mant * (1.0 / 9007199254740992.0);
+    if (mode == DV_SAMPLE_STRATIFIED) u = ((double)q + u) / (double)M;  // stratum q of M
+    double y = u * run;
     int k = (int)(std::upper_bound(cdf.begin(), cdf.end(), y) - cdf.begin()) - 1;
     if (k < 0) k = 0;
     while (k > 0 && !(s->kden[c->targets[k]] > 0.0f)) --k;

@@ -216,11 +216,15 @@ def test_inverse_cdf_sampler_matches_oracle(cuda, channel):
     o = mirror(ps)
     resort_identity(o)
     M = 700
-    from dimcv_sph_b200._abi import DV_SAMPLE_INVERSE_CDF
-    solver._calls("dv_sample", DV_SAMPLE_INVERSE_CDF, 11, 3, M)
-    o.calls("sample", DV_SAMPLE_INVERSE_CDF, 11, 3, M)
-    assert ps.counters()["num_samples"] == M
-    bitexact(solver.sample_idx[:M].cpu().numpy(), o.solver["sample_idx"][:M], "inverse-CDF draws")
+    from dimcv_sph_b200._abi import DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED
+    for mode in (DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED):
+        solver._calls("dv_sample", mode, 11, 3, M)
+        o.calls("sample", mode, 11, 3, M)
+        assert ps.counters()["num_samples"] == M
+        bitexact(solver.sample_idx[:M].cpu().numpy(), o.solver["sample_idx"][:M], f"draws (mode {mode})")
+    # stratified draws are non-decreasing in CDF order (slot order of the targets)
+    d = solver.sample_idx[:M].cpu().numpy()
+    assert np.all(np.diff(d) >= 0)
 
 
 @pytest.mark.parametrize("compensated", [False, True])
