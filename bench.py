@@ -262,7 +262,7 @@ def run_ours(args, rank, world, local):
     achieved = FLOPS_PER_PAIR[dim] * pairs.value / (far_ms.value * 1e-3) / 1e12 if far_ms.value > 0 else 0.0
     peak_tf = peak.value / 1e12
     traffic = read_traffic()
-    roofline = {"kernel": "k_vvpe_far (Monte-Carlo Biot-Savart far field)", "bound": "fp32",
+    roofline = {"kernel": "k_far_main (Monte-Carlo Biot-Savart far field)", "bound": "fp32",
                 "achieved": round(achieved, 3), "peak": round(peak_tf, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_tf, 4) if peak_tf else None,
                 "traffic": traffic,
@@ -278,7 +278,8 @@ def run_ours(args, rank, world, local):
                              num_samples=cnt1["num_samples"], parallelism=f"replicas x{world}",
                              l2="state (~1.3 GB) larger than L2; no flush"),
               "clocks": clk, "gpu_launches": int(launches), "roofline": roofline,
-              "iterations": {"divergence": cnt1["iters_div"], "pressure": cnt1["iters_p"]}}
+              "iterations": {"divergence": cnt1["iters_div"], "pressure": cnt1["iters_p"]},
+              "far_tile_targets_per_thread": solver.far_tile}
 
     # per-stage device times and HBM fractions (outside the timed region)
     st = stage_times(solver, ps, 3)

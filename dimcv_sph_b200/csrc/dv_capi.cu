@@ -104,7 +104,7 @@ DV_API void dv_destroy(dv_ctx* c) {
                   c->hist,    c->cell_start, c->cell_end, c->mt[0],     c->mt[1],   c->mt[2],
                   c->scan_part, c->dscan_part, c->red_part, c->ired_part, c->flags, c->offs,
                   c->targets, c->cdf,       c->spos,      c->sw,        c->near_v,  c->near_S,
-                  c->far_acc, c->mult};
+                  c->far_acc, c->mult,      c->nbr_off,   c->nbr_idx,   c->d_nbr_ok};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2 * dv_ctx::kProfPool; ++k)
@@ -170,6 +170,12 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   A(c->near_S, cap);
   A(c->far_acc, cap);
   A(c->mult, cap);
+  // neighbour lists: 48 (3-D) / 24 (2-D) entries per particle on average,
+  // beyond which the sweeps keep scanning cells
+  c->nbr_cap = cap * (params->dim == 3 ? 48 : 24);
+  A(c->nbr_off, cap + 1);
+  A(c->nbr_idx, c->nbr_cap);
+  A(c->d_nbr_ok, 1);
   A(c->d_prof, 4);
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_cnt, sizeof(dv_counters));
@@ -177,6 +183,7 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   if (e == cudaSuccess) e = cudaMemset(c->d_cnt, 0, sizeof(dv_counters));
   if (e == cudaSuccess) e = cudaMemset(c->d_flag, 0, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(c->d_prof, 0, sizeof(double) * 4);
+  if (e == cudaSuccess) e = cudaMemset(c->d_nbr_ok, 0, sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMemset(c->cell_start, 0, sizeof(int32_t) * c->ncells);
   if (e == cudaSuccess) e = cudaMemset(c->cell_end, 0, sizeof(int32_t) * c->ncells);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -212,7 +219,7 @@ DV_API int dv_set_counts(dv_ctx* c, int32_t n, int32_t n_fluid, int32_t n_solid)
   k_set_counts<<<1, 1, 0, c->stream>>>(c->d_cnt, n, n_fluid, n_solid);
   DV_LAUNCHED(c);
   c->n_upper = n;
-  return DV_OK;
+  return dv_invalidate_lists(c);
 }
 
 __global__ void k_clear_status(dv_counters* C) { C->status = 0; }

@@ -254,6 +254,64 @@ __global__ void k_finalize_counts(const int32_t* __restrict__ part, int nparts,
   }
 }
 
+// ------------------------------------------------- per-step neighbour lists
+// After the sort, every sweep of the step visits the same neighbour sets in
+// the same order, so the cell scan (3^d cells, ~8 candidates each in 3-D) is
+// done once here and the sweeps read the lists.  count -> scan -> fill.
+template <int D>
+__global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
+                            const dv_counters* __restrict__ C, int m, uint32_t* __restrict__ cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  uint32_t k = 0;
+  if (i < C->n) for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int, V3, float) { ++k; });
+  cnt[i] = k;
+}
+
+__global__ void k_csr_ok(const uint32_t* __restrict__ off, const dv_counters* __restrict__ C, int64_t cap,
+                         int32_t* __restrict__ ok) {
+  *ok = (int64_t)off[C->n] <= cap ? 1 : 0;
+}
+
+template <int D>
+__global__ void k_csr_fill(dv_params P, DevGrid G, const float* __restrict__ x,
+                           const dv_counters* __restrict__ C, const uint32_t* __restrict__ off,
+                           const int32_t* __restrict__ ok, int32_t* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C->n || !*ok) return;
+  uint32_t k = off[i];
+  for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) { out[k++] = j; });
+}
+
+static int build_csr(dv_ctx* c, const dv_fields* f) {
+  const int m = (int)std::min<int64_t>(c->n_upper, c->cap) + 1;
+  const int nb = dv_blocks(m);
+  DevGrid G = dv_grid_cells(c);
+  if (c->p.dim == 2)
+    k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
+  else
+    k_csr_count<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
+  DV_LAUNCHED(c);
+  int rc = dv_scan_u32(c, c->flags, c->nbr_off, m);
+  if (rc) return rc;
+  k_csr_ok<<<1, 1, 0, c->stream>>>(c->nbr_off, c->d_cnt, c->nbr_cap, c->d_nbr_ok);
+  DV_LAUNCHED(c);
+  if (c->p.dim == 2)
+    k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
+                                                    c->nbr_idx);
+  else
+    k_csr_fill<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
+                                                    c->nbr_idx);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+// positions or the particle count changed: sweeps go back to the cell scan
+int dv_invalidate_lists(dv_ctx* c) {
+  DV_CK(c, cudaMemsetAsync(c->d_nbr_ok, 0, sizeof(int32_t), c->stream));
+  return DV_OK;
+}
+
 static int check_fields(dv_ctx* c, const dv_fields* f, const char* who) {
   if (!f->x || !f->x0 || !f->v || !f->acceleration || !f->vorticity || !f->m_V || !f->m ||
       !f->density || !f->pressure || !f->dfsph_factor || !f->density_adv || !f->life_time ||
@@ -274,7 +332,9 @@ DV_API int dv_grid_build(dv_ctx* c, const dv_fields* src, const dv_fields* dst) 
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const uint32_t invalid = (c->kbits >= 32) ? 0xffffffffu : ((1u << c->kbits) - 1u);
   const int nb = dv_blocks(nu);
-  DevGrid G = dv_grid(c);
+  rc = dv_invalidate_lists(c);
+  if (rc) return rc;
+  DevGrid G = dv_grid_cells(c);
   if (c->p.dim == 2)
     k_cell_keys<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *src, G, c->d_cnt, c->keys[0], invalid);
   else
@@ -313,7 +373,7 @@ DV_API int dv_grid_build(dv_ctx* c, const dv_fields* src, const dv_fields* dst) 
   DV_LAUNCHED(c);
   k_finalize_counts<<<1, 1024, 0, c->stream>>>(c->ired_part, nb, c->d_flag + 1, c->d_cnt);
   DV_LAUNCHED(c);
-  return DV_OK;
+  return build_csr(c, dst);
 }
 
 DV_API int dv_get_permutation(dv_ctx* c, int32_t* host_perm, int64_t n_cap) {
@@ -395,7 +455,7 @@ DV_API int dv_add_particles(dv_ctx* c, const dv_fields* f, const float* pos, con
   k_add_counts<<<1, 1, 0, c->stream>>>(c->d_cnt, count, (int)c->cap, material);
   DV_LAUNCHED(c);
   c->n_upper = std::min<int64_t>(c->n_upper + count, c->cap);
-  return DV_OK;
+  return dv_invalidate_lists(c);
 }
 
 // ----------------------------------------------------------- neighbour CSR
@@ -431,7 +491,8 @@ DV_API int64_t dv_neighbor_lists(dv_ctx* c, const dv_fields* f, int64_t* dev_off
   int rc = dv_get_counters(c, &cnt);
   if (rc) return rc;
   const int n = cnt.n;
-  DevGrid G = dv_grid(c);
+  // always the cell scan: this entry point checks the lists the sweeps use
+  DevGrid G = dv_grid_cells(c);
   int nb = dv_blocks(n);
   if (c->p.dim == 2)
     k_nbr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->flags);

@@ -67,6 +67,12 @@ struct dv_ctx {
   int32_t* mult = nullptr;     // cap: sample multiplicity per slot
   int far_tt = 4;              // targets per thread of the far-field main loop (autotuned)
 
+  // per-step neighbour lists (CSR, visit order) built by dv_grid_build
+  uint32_t* nbr_off = nullptr;  // cap + 1
+  int32_t* nbr_idx = nullptr;   // nbr_cap
+  int64_t nbr_cap = 0;
+  int32_t* d_nbr_ok = nullptr;  // 1 while the lists match the current positions
+
   // far-field kernel profiling (dv_profile)
   bool prof = false;
   static constexpr int kProfPool = 512;
@@ -103,9 +109,19 @@ struct DevGrid {
   const uint32_t* mt0;
   const uint32_t* mt1;
   const uint32_t* mt2;
+  // neighbour lists of the last grid build (CSR in visit order); used while
+  // *nok != 0, i.e. until positions move or particles are added
+  const uint32_t* noff;
+  const int32_t* nidx;
+  const int32_t* nok;
 };
 static inline DevGrid dv_grid(const dv_ctx* c) {
-  return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2]};
+  return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2], c->nbr_off, c->nbr_idx,
+                 c->d_nbr_ok};
+}
+// the cell-scan form only (used to build the neighbour lists)
+static inline DevGrid dv_grid_cells(const dv_ctx* c) {
+  return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2], nullptr, nullptr, nullptr};
 }
 
 // ------------------------------------------------------------- scan helpers
@@ -115,6 +131,8 @@ int dv_scan_u32(dv_ctx* c, const uint32_t* in, uint32_t* out, int64_t m);
 int dv_scan_f64(dv_ctx* c, const double* in, double* out, int64_t m);
 // Sum of `nparts` FP64 partials into *dst (device), one block, fixed order.
 int dv_finalize_sum(dv_ctx* c, const double* parts, int nparts, double* dst);
+// Marks the per-step neighbour lists stale (positions or counts changed).
+int dv_invalidate_lists(dv_ctx* c);
 
 // ------------------------------------------------------------ device helpers
 struct V3 {
@@ -193,7 +211,10 @@ __device__ __forceinline__ V3 cubic_gradW(const dv_params& P, V3 r, float r2) {
   float r_norm = sqrtf(r2);
   float q = r_norm * h;
   if (r_norm > P.grad_r_min && q <= 1.0f) {
-    V3 gq{(r.x / r_norm) * h, (r.y / r_norm) * h, D == 3 ? (r.z / r_norm) * h : 0.0f};
+    // r / r_norm * h with the division as one IEEE reciprocal (the arcp form
+    // of the reference's fast-math codegen); the oracle does the same
+    const float inv = 1.0f / r_norm;
+    V3 gq{(r.x * inv) * h, (r.y * inv) * h, D == 3 ? (r.z * inv) * h : 0.0f};
     float s;
     if (q <= 0.5f) {
       s = (P.kG * q) * (3.0f * q - 2.0f);
@@ -246,6 +267,17 @@ template <int D, typename F>
 __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevGrid& G,
                                                   const float* __restrict__ x, int i, V3 xi,
                                                   F&& f) {
+  if (G.nok && __ldg(G.nok)) {  // the lists hold exactly these j, in this order
+    const uint32_t k1 = __ldg(G.noff + i + 1);
+#pragma unroll 1
+    for (uint32_t k = __ldg(G.noff + i); k < k1; ++k) {
+      const int j = __ldg(G.nidx + k);
+      V3 xj = ldv<D>(x, j);
+      V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
+      f(j, r, sqnorm<D>(r));
+    }
+    return;
+  }
   int c0 = cell_coord(P, xi.x, 0), c1 = cell_coord(P, xi.y, 1);
   int c2 = D == 3 ? cell_coord(P, xi.z, 2) : 0;
   const float lim = P.nbr_r2_limit;

@@ -539,5 +539,5 @@ DV_API int dv_predict_velocity(dv_ctx* c, const dv_fields* f) {
 DV_API int dv_advect(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_advect, nblk(c), c->p, *f, c->d_cnt);
-  return DV_OK;
+  return dv_invalidate_lists(c);  // positions moved
 }

@@ -91,7 +91,7 @@ class RingStudy:
         return e0.elapsed_time(e1) / reps
 
 
-def run(n=1 << 20, Ms=(4096, 16384, 65536, 131072), seeds=3, subset=262144, reps=3, target_err=0.02,
+def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=3, subset=262144, reps=3, target_err=0.02,
         device="cuda") -> dict:
     st = RingStudy(n=n, subset=subset, device=device)
     out = {"n": n, "subset": int(st.sub.numel()), "kernel": "blob3d (1/4π) V (r×ω)/(|r|²+δ²)^{3/2}, δ = r",

@@ -125,7 +125,10 @@ inline V cubic_kernel_derivative(const Ctx& c, V r) {
   float q = r_norm * h;
   V res;
   if (r_norm > P.grad_r_min && q <= 1.0f) {
-    V gq{r.x / r_norm * h, r.y / r_norm * h, c.p.dim == 3 ? r.z / r_norm * h : 0.0f};
+    // `r / r_norm * h` with the division taken as one reciprocal, the form
+    // Taichi's default fast-math (arcp) codegen is allowed to emit
+    const float inv = 1.0f / r_norm;
+    V gq{r.x * inv * h, r.y * inv * h, c.p.dim == 3 ? r.z * inv * h : 0.0f};
     float s;
     if (q <= 0.5f) {
       s = k * q * (3.0f * q - 2.0f);
