@@ -84,7 +84,9 @@ class DvParams(C.Structure):
         ("blob_delta2", C.c_float),
         ("blob_coef", C.c_float),
         ("compensated", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("periodic", C.c_int32),
+        ("box", F3),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -128,6 +128,22 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
     dv_fail(nullptr, DV_EINVAL, "capacity %lld out of range [1, 2^30]", (long long)capacity);
     return nullptr;
   }
+  if (params->periodic) {
+    if (!params->cell_origin_offset) {
+      dv_fail(nullptr, DV_EINVAL, "periodic boxes need cell_origin_offset = 1");
+      return nullptr;
+    }
+    for (int d = 0; d < params->dim; ++d) {
+      const double cells = (double)params->box[d] / (double)params->grid_size;
+      if (params->grid_num[d] < 5 || fabs(cells - params->grid_num[d]) > 1e-4 * params->grid_num[d] ||
+          params->grid_size < params->support_radius) {
+        dv_fail(nullptr, DV_EINVAL,
+                "periodic axis %d: need >= 5 cells of size box/grid_num >= h (box %g, grid_size %g, %d cells)", d,
+                (double)params->box[d], (double)params->grid_size, params->grid_num[d]);
+        return nullptr;
+      }
+    }
+  }
   dv_ctx* c = new dv_ctx();
   c->p = *params;
   c->cap = capacity;

@@ -19,7 +19,7 @@ __global__ void k_update_activity(dv_params P, dv_fields F, const dv_counters* _
   int mat = F.material[i];
   if (mat == DV_MATERIAL_SOLID) {
     F.is_active[i] = 1;
-  } else if (mat == DV_MATERIAL_FLUID) {
+  } else if (mat == DV_MATERIAL_FLUID && !P.periodic) {  // nothing leaves a periodic box
     V3 x = ldv<D>(F.x, i);
     bool out = x.x < P.domain_start[0] || x.x > P.domain_end[0] || x.y < P.domain_start[1] ||
                x.y > P.domain_end[1];

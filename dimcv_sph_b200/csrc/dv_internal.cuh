@@ -237,7 +237,34 @@ __device__ __forceinline__ int cell_coord(const dv_params& P, float x, int d) {
   float q = t / P.grid_size;
   if (!(q > -1.0e9f)) q = -1.0e9f;
   if (q > 1.0e9f) q = 1.0e9f;
-  return (int)q;
+  int g = (int)q;
+  // a periodic box holds every position in [start, start + box): a quotient
+  // that rounds up to grid_num belongs to the last cell
+  if (P.periodic) g = g < 0 ? 0 : (g >= P.grid_num[d] ? P.grid_num[d] - 1 : g);
+  return g;
+}
+
+// minimum-image difference on a periodic axis of length L (|d| < L assumed)
+__device__ __forceinline__ float min_image(float d, float L) {
+  const float hl = 0.5f * L;
+  return d > hl ? __fsub_rn(d, L) : (d < -hl ? __fadd_rn(d, L) : d);
+}
+// r = x_i - x_j, minimum image when the box is periodic
+template <int D>
+__device__ __forceinline__ V3 rel(const dv_params& P, V3 xi, V3 xj) {
+  V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
+  if (P.periodic) {
+    r.x = min_image(r.x, P.box[0]);
+    r.y = min_image(r.y, P.box[1]);
+    if (D == 3) r.z = min_image(r.z, P.box[2]);
+  }
+  return r;
+}
+// cell coordinate c + a on an axis of n cells: wrapped when periodic, -1 if outside
+__device__ __forceinline__ int cell_step(const dv_params& P, int c, int a, int n) {
+  int g = c + a;
+  if (P.periodic) return g < 0 ? g + n : (g >= n ? g - n : g);
+  return (g < 0 || g >= n) ? -1 : g;
 }
 
 template <int D>
@@ -272,8 +299,7 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
 #pragma unroll 1
     for (uint32_t k = __ldg(G.noff + i); k < k1; ++k) {
       const int j = __ldg(G.nidx + k);
-      V3 xj = ldv<D>(x, j);
-      V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
+      V3 r = rel<D>(P, xi, ldv<D>(x, j));
       f(j, r, sqnorm<D>(r));
     }
     return;
@@ -283,20 +309,20 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
   const float lim = P.nbr_r2_limit;
 #pragma unroll 1
   for (int a = -1; a <= 1; ++a) {
-    int gx = c0 + a;
-    if (gx < 0 || gx >= P.grid_num[0]) continue;
+    int gx = cell_step(P, c0, a, P.grid_num[0]);
+    if (gx < 0) continue;
     uint32_t kx = __ldg(G.mt0 + gx);
 #pragma unroll 1
     for (int b = -1; b <= 1; ++b) {
-      int gy = c1 + b;
-      if (gy < 0 || gy >= P.grid_num[1]) continue;
+      int gy = cell_step(P, c1, b, P.grid_num[1]);
+      if (gy < 0) continue;
       uint32_t kxy = kx | __ldg(G.mt1 + gy);
 #pragma unroll 1
       for (int c = (D == 3 ? -1 : 0); c <= (D == 3 ? 1 : 0); ++c) {
         uint32_t key = kxy;
         if (D == 3) {
-          int gz = c2 + c;
-          if (gz < 0 || gz >= P.grid_num[2]) continue;
+          int gz = cell_step(P, c2, c, P.grid_num[2]);
+          if (gz < 0) continue;
           key |= __ldg(G.mt2 + gz);
         }
         if (P.skip_cell0 && key == 0u) continue;
@@ -304,8 +330,7 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
 #pragma unroll 1
         for (int j = s; j < e; ++j) {
           if (j == i) continue;
-          V3 xj = ldv<D>(x, j);
-          V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
+          V3 r = rel<D>(P, xi, ldv<D>(x, j));
           float r2 = sqnorm<D>(r);
           if (r2 < lim) f(j, r, r2);
         }

@@ -376,6 +376,17 @@ __global__ void k_advect(dv_params P, dv_fields F, const dv_counters* __restrict
   x.x += P.dt * v.x;
   x.y += P.dt * v.y;
   if (D == 3) x.z += P.dt * v.z;
+  if (P.periodic) {  // wrap into [domain_start, domain_start + box)
+    float* c[3] = {&x.x, &x.y, &x.z};
+    for (int d = 0; d < D; ++d) {
+      if (*c[d] >= P.domain_start[d] + P.box[d]) *c[d] -= P.box[d];
+      if (*c[d] < P.domain_start[d]) {
+        *c[d] += P.box[d];
+        // -tiny + box rounds to box: that point is the start of the axis
+        if (*c[d] >= P.domain_start[d] + P.box[d]) *c[d] = P.domain_start[d];
+      }
+    }
+  }
   stv<D>(F.x, i, x);
 }
 

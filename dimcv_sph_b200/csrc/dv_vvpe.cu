@@ -223,13 +223,20 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// coordinate difference, minimum image on a periodic box
+template <bool PER>
+__device__ __forceinline__ float wrapd(float d, float L) {
+  return PER ? min_image(d, L) : d;
+}
+
 // one pair of the main loop: returns the three increments (r × ω̂ weighted)
-template <int D, bool BLOB>
+template <int D, bool BLOB, bool PER = false>
 __device__ __forceinline__ void far_terms(float px, float py, float pz, float4 sp, float4 w, float lim,
-                                          float d2, float& cx, float& cy, float& cz) {
-  const float dx = __fsub_rn(px, sp.x);
-  const float dy = __fsub_rn(py, sp.y);
-  const float dz = D == 3 ? __fsub_rn(pz, sp.z) : 0.0f;
+                                          float d2, float& cx, float& cy, float& cz,
+                                          float3 bx = float3{0.f, 0.f, 0.f}) {
+  const float dx = wrapd<PER>(__fsub_rn(px, sp.x), bx.x);
+  const float dy = wrapd<PER>(__fsub_rn(py, sp.y), bx.y);
+  const float dz = D == 3 ? wrapd<PER>(__fsub_rn(pz, sp.z), bx.z) : 0.0f;
   float r2 = __fmul_rn(dx, dx);
   r2 = __fmaf_rn(dy, dy, r2);
   if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
@@ -251,18 +258,19 @@ __device__ __forceinline__ void far_terms(float px, float py, float pz, float4 s
 }
 
 // main loop accumulation form of far_terms (lets the increments fuse into FMAs)
-template <int D, bool BLOB, bool COMP>
+template <int D, bool BLOB, bool COMP, bool PER = false>
 __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 sp, float4 w, float lim, float d2,
-                                          Acc<COMP>& ax, Acc<COMP>& ay, Acc<COMP>& az) {
-  const float dx = __fsub_rn(px, sp.x);
-  const float dy = __fsub_rn(py, sp.y);
-  const float dz = D == 3 ? __fsub_rn(pz, sp.z) : 0.0f;
+                                          Acc<COMP>& ax, Acc<COMP>& ay, Acc<COMP>& az,
+                                          float3 bx = float3{0.f, 0.f, 0.f}) {
+  const float dx = wrapd<PER>(__fsub_rn(px, sp.x), bx.x);
+  const float dy = wrapd<PER>(__fsub_rn(py, sp.y), bx.y);
+  const float dz = D == 3 ? wrapd<PER>(__fsub_rn(pz, sp.z), bx.z) : 0.0f;
   float r2 = __fmul_rn(dx, dx);
   r2 = __fmaf_rn(dy, dy, r2);
   if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
   if (COMP) {
     float cx, cy, cz;
-    far_terms<D, BLOB>(px, py, pz, sp, w, lim, d2, cx, cy, cz);
+    far_terms<D, BLOB, PER>(px, py, pz, sp, w, lim, d2, cx, cy, cz, bx);
     ax.add(cx);
     ay.add(cy);
     az.add(cz);
@@ -289,7 +297,7 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
 #define FT2 256
 #define FTILE2 512
 
-template <int D, int TT, bool BLOB, bool COMP>
+template <int D, int TT, bool BLOB, bool COMP, bool PER>
 __global__ void __launch_bounds__(FT2) k_far_main(dv_params P, const float* __restrict__ x,
                                                   const dv_counters* __restrict__ C,
                                                   const int32_t* __restrict__ targets,
@@ -314,6 +322,7 @@ __global__ void __launch_bounds__(FT2) k_far_main(dv_params P, const float* __re
   }
   const float lim = P.far_r2_limit;
   const float d2 = P.blob_delta2;
+  const float3 bx = make_float3(P.box[0], P.box[1], P.box[2]);
   for (int base = 0; base < M; base += FTILE2) {
     const int m = min(FTILE2, M - base);
     __syncthreads();
@@ -327,7 +336,8 @@ __global__ void __launch_bounds__(FT2) k_far_main(dv_params P, const float* __re
       const float4 sp = s_p[q];
       const float4 w = s_w[q];
 #pragma unroll
-      for (int k = 0; k < TT; ++k) far_accum<D, BLOB, COMP>(px[k], py[k], pz[k], sp, w, lim, d2, ax[k], ay[k], az[k]);
+      for (int k = 0; k < TT; ++k)
+        far_accum<D, BLOB, COMP, PER>(px[k], py[k], pz[k], sp, w, lim, d2, ax[k], ay[k], az[k], bx);
     }
   }
 #pragma unroll
@@ -350,7 +360,8 @@ __global__ void k_mult(const int32_t* __restrict__ sample_idx, const dv_counters
 // cell window of a target that contains every particle within h: the 3^d
 // cells around its cell, widened by one cell on a side where the target's
 // cell coordinate is within rounding of a cell face (a particle exactly h
-// away can then sit two cells over)
+// away can then sit two cells over).  On a periodic axis the window wraps
+// (lo/hi are then offsets to be wrapped by cell_step, see k_far_fix).
 __device__ __forceinline__ void far_window(const dv_params& P, float xv, int d, int& lo, int& hi) {
   float t = P.cell_origin_offset ? (xv - P.domain_start[d]) : xv;
   float q = t / P.grid_size;
@@ -359,11 +370,19 @@ __device__ __forceinline__ void far_window(const dv_params& P, float xv, int d, 
   float frac = q - (float)c;
   lo = c - 1 - (frac <= tol ? 1 : 0);
   hi = c + 1 + (frac >= 1.0f - tol ? 1 : 0);
-  lo = max(lo, 0);
-  hi = min(hi, P.grid_num[d] - 1);
+  if (!P.periodic) {
+    lo = max(lo, 0);
+    hi = min(hi, P.grid_num[d] - 1);
+  }
 }
 
-template <int D, bool BLOB>
+__device__ __forceinline__ int wrap_cell(const dv_params& P, int g, int d) {
+  if (!P.periodic) return g;
+  const int n = P.grid_num[d];
+  return g < 0 ? g + n : (g >= n ? g - n : g);
+}
+
+template <int D, bool BLOB, bool PER>
 __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
                           const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
                           const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
@@ -375,6 +394,7 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
   const int i = targets[t];
   const V3 xi = ldv<D>(F.x, i);
   const float lim = P.far_r2_limit, d2 = P.blob_delta2;
+  const float3 bx = make_float3(P.box[0], P.box[1], P.box[2]);
   float4 acc = far_acc[t];
   int near_cnt = 0;
   int lo0, hi0, lo1, hi1, lo2 = 0, hi2 = 0;
@@ -382,24 +402,24 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
   far_window(P, xi.y, 1, lo1, hi1);
   if (D == 3) far_window(P, xi.z, 2, lo2, hi2);
   for (int a = lo0; a <= hi0; ++a) {
-    const uint32_t ka = __ldg(G.mt0 + a);
+    const uint32_t ka = __ldg(G.mt0 + wrap_cell(P, a, 0));
     for (int b = lo1; b <= hi1; ++b) {
-      const uint32_t kab = ka | __ldg(G.mt1 + b);
+      const uint32_t kab = ka | __ldg(G.mt1 + wrap_cell(P, b, 1));
       for (int cc = lo2; cc <= hi2; ++cc) {
-        const uint32_t key = D == 3 ? (kab | __ldg(G.mt2 + cc)) : kab;
+        const uint32_t key = D == 3 ? (kab | __ldg(G.mt2 + wrap_cell(P, cc, 2))) : kab;
         const int s0 = __ldg(G.start + key), e0 = __ldg(G.end + key);
         for (int j = s0; j < e0; ++j) {
           const int m = mult[j];
           if (m == 0) continue;
           const V3 xj = ldv<D>(F.x, j);
-          V3 r{__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), D == 3 ? __fsub_rn(xi.z, xj.z) : 0.0f};
-          if (sqnorm<D>(r) > lim) continue;  // far: the main loop's term stays
+          if (sqnorm<D>(rel<D>(P, xi, xj)) > lim) continue;  // far: the main loop's term stays
           near_cnt += m;
           const V3 w3 = ld4(S.d_vort_smoothed, j);
           const float inv = 1.0f / (S.kden[j] + P.kden_eps);
           const float4 w = make_float4(w3.x * inv, w3.y * inv, w3.z * inv, 0.0f);
           float cx, cy, cz;
-          far_terms<D, BLOB>(xi.x, xi.y, xi.z, make_float4(xj.x, xj.y, xj.z, 0.0f), w, lim, d2, cx, cy, cz);
+          far_terms<D, BLOB, PER>(xi.x, xi.y, xi.z, make_float4(xj.x, xj.y, xj.z, 0.0f), w, lim, d2, cx, cy,
+                                  cz, bx);
           const float fm = (float)m;
           acc.x = __fmaf_rn(-fm, cx, acc.x);
           acc.y = __fmaf_rn(-fm, cy, acc.y);
@@ -433,13 +453,13 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
   }
 }
 
-template <int D, bool BLOB, bool COMP>
+template <int D, bool BLOB, bool COMP, bool PER>
 static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const int nb = (int)std::max<int64_t>(1, (nu + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
-#define L(TTV)                                                                                          \
-  k_far_main<D, TTV, BLOB, COMP><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
-                                                            c->sw, c->far_acc)
+#define L(TTV)                                                                                               \
+  k_far_main<D, TTV, BLOB, COMP, PER><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
+                                                                 c->sw, c->far_acc)
   if (tt <= 2)
     L(2);
   else if (tt <= 4)
@@ -449,25 +469,36 @@ static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
 #undef L
 }
 
-template <int D>
-static void launch_main(dv_ctx* c, const dv_fields* f, int tt) {
+template <int D, bool PER>
+static void launch_main_p(dv_ctx* c, const dv_fields* f, int tt) {
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   const bool comp = c->p.compensated != 0;
   if (blob)
-    comp ? launch_main_tt<D, true, true>(c, f, tt) : launch_main_tt<D, true, false>(c, f, tt);
+    comp ? launch_main_tt<D, true, true, PER>(c, f, tt) : launch_main_tt<D, true, false, PER>(c, f, tt);
   else
-    comp ? launch_main_tt<D, false, true>(c, f, tt) : launch_main_tt<D, false, false>(c, f, tt);
+    comp ? launch_main_tt<D, false, true, PER>(c, f, tt) : launch_main_tt<D, false, false, PER>(c, f, tt);
+}
+
+template <int D>
+static void launch_main(dv_ctx* c, const dv_fields* f, int tt) {
+  if (c->p.periodic)
+    launch_main_p<D, true>(c, f, tt);
+  else
+    launch_main_p<D, false>(c, f, tt);
 }
 
 template <int D>
 static void launch_fix(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   const int nb = dv_blocks(std::min<int64_t>(c->n_upper, c->cap), 128);
-  if (c->p.kernel_mode == DV_KERNEL_BLOB3D)
-    k_far_fix<D, true><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,
-                                                  c->far_acc, c->near_v, c->near_S);
+#define LF(B, PR)                                                                                      \
+  k_far_fix<D, B, PR><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult, \
+                                                 c->far_acc, c->near_v, c->near_S)
+  const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  if (c->p.periodic)
+    blob ? LF(true, true) : LF(false, true);
   else
-    k_far_fix<D, false><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,
-                                                   c->far_acc, c->near_v, c->near_S);
+    blob ? LF(true, false) : LF(false, false);
+#undef LF
 }
 
 __global__ void k_prof_pairs(const dv_counters* __restrict__ C, double* acc) {
@@ -581,6 +612,8 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
   DV_LAUNCHED(c);
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const bool fastk = fast_kernel_ok(c->p) || c->p.kernel_mode == DV_KERNEL_BLOB3D;
+  if (!fastk && c->p.periodic)
+    return dv_fail(c, DV_EUNSUPPORTED, "dv_vvpe_mc: periodic boxes need h > 1.05e-4 (reference kernel)");
   if (fastk) {  // split form: sample multiplicities for the correction kernel
     DV_CK(c, cudaMemsetAsync(c->mult, 0, sizeof(int32_t) * nu, c->stream));
     k_mult<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(s->sample_idx, c->d_cnt, c->mult);
@@ -699,6 +732,12 @@ __global__ void __launch_bounds__(FT) k_bs_full(dv_params P, const float* __rest
       if (__float_as_int(sp.w) == i) continue;
       const float4 w = s_w[q];
       T dx = px - (T)sp.x, dy = py - (T)sp.y, dz = D == 3 ? pz - (T)sp.z : (T)0;
+      if (P.periodic) {  // minimum image
+        const T L0 = (T)P.box[0], L1 = (T)P.box[1], L2 = (T)P.box[2];
+        dx = dx > L0 / 2 ? dx - L0 : (dx < -L0 / 2 ? dx + L0 : dx);
+        dy = dy > L1 / 2 ? dy - L1 : (dy < -L1 / 2 ? dy + L1 : dy);
+        if (D == 3) dz = dz > L2 / 2 ? dz - L2 : (dz < -L2 / 2 ? dz + L2 : dz);
+      }
       T r2 = dx * dx + dy * dy + dz * dz;
       if (r2 == (T)0) continue;
       if (!BLOB) {
@@ -794,7 +833,7 @@ static int bs_dispatch(dv_ctx* c, const dv_fields* f, const int32_t* targets, in
   const int nb = dv_blocks(nt, FT);
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   const int32_t* ns = c->d_flag + 2;
-  if (precision == 32 && blob) {
+  if (precision == 32 && blob && !c->p.periodic) {
     const int tt = c->far_tt <= 2 ? 2 : (c->far_tt <= 4 ? 4 : 8);
     const int nbf = (int)std::max<int64_t>(1, ((int64_t)nt + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
 #define LBS(TTV, CV)                                                                                          \

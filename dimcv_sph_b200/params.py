@@ -60,6 +60,7 @@ class Options:
     kernel: str = "ref2d"            # "ref2d" (dimcv_sph.py:649-719) | "blob3d"
     blob_delta: float | None = None  # regularisation radius of blob3d (default: particle radius)
     compensated: bool = False        # compensated f32 accumulation in the N-body sums
+    periodic: bool = False           # every axis wraps; minimum-image distances
     extra: dict = field(default_factory=dict)
 
     @classmethod
@@ -76,6 +77,8 @@ class Options:
             o.blob_delta = float(g("blobDelta"))
         if g("compensated") is not None:
             o.compensated = bool(g("compensated"))
+        if g("periodic") is not None:
+            o.periodic = bool(g("periodic"))
         return o
 
 
@@ -160,6 +163,22 @@ def make_params(cfg, options: Options | None = None) -> DvParams:
     p.blob_delta2 = f32(delta * delta)
     p.blob_coef = f32(vp_volume / (4.0 * math.pi))
     p.compensated = 1 if o.compensated else 0
+    if o.periodic:
+        # cells of size box / floor(box / h) >= h, the same on every axis, so
+        # the 3^d window around a cell holds every minimum-image neighbour
+        n_cells = np.floor(domain_size / support).astype(int)
+        gs = domain_size[0] / n_cells[0]
+        for d in range(dim):
+            if abs(domain_size[d] / n_cells[d] - gs) > 1e-9 * gs:
+                raise ValueError("a periodic box needs the same cell size box/floor(box/h) on every axis")
+            if n_cells[d] < 5:
+                raise ValueError("a periodic box needs at least 5 cells per axis")
+            p.grid_num[d] = int(n_cells[d])
+            p.box[d] = f32(domain_size[d])
+        p.grid_size = f32(gs)
+        p.periodic = 1
+        p.cell_origin_offset = 1
+        p.skip_cell0 = 0
     return p
 
 

@@ -114,6 +114,49 @@ def sphere3d(radius=0.004, size=(3.0, 1.0, 1.0), inflow=1.0, center=(0.5, 0.5, 0
     return SimConfig(config=cfg)
 
 
+def periodic_blobs(x: np.ndarray, seed: int, n_blobs=8) -> np.ndarray:
+    """Vorticity (z) of n_blobs Gaussian blobs on the unit periodic square:
+    amplitude N(0, 5), width σ ~ U(0.03, 0.08), centres uniform; distances
+    by minimum image."""
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(0.0, 1.0, size=(n_blobs, 2))
+    amps = rng.normal(0.0, 5.0, size=n_blobs)
+    sig = rng.uniform(0.03, 0.08, size=n_blobs)
+    w = np.zeros(x.shape[0])
+    for c, a, s in zip(centers, amps, sig):
+        d = x[:, :2] - c
+        d -= np.round(d)
+        w += a * np.exp(-(d * d).sum(1) / (s * s))
+    return w
+
+
+def periodic2d(n: int = 65536, seed: int = 0, jitter: float = 0.25, dt: float = 1e-3):
+    """(config, positions float32 [n,2], vorticity float32 [n]) on the unit
+    periodic square: a jittered √n × √n lattice (jitter U(-j, j)·spacing),
+    particle radius = spacing / 2 (h = 2 spacings), volume 1/n per particle."""
+    k = int(round(math.sqrt(n)))
+    if k * k != n:
+        raise ValueError("n must be a square number")
+    sp = 1.0 / k
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(k), np.arange(k), indexing="ij"), -1).reshape(-1, 2)
+    x = (g + 0.5) * sp + rng.uniform(-jitter, jitter, size=g.shape) * sp
+    x = np.mod(x, 1.0)
+    w = periodic_blobs(x, seed + 1)
+    cfg = {
+        "Configuration": {
+            "domainStart": [0.0, 0.0], "domainEnd": [1.0, 1.0], "particleRadius": sp / 2,
+            "density0": 1000, "simulationMethod": 0, "gravitation": [0.0, 0.0], "timeStepSize": dt,
+            # vp_volume = volumeScale * 0.8 (2r)^2 = 1/n
+            "volumeScale": 1.25, "GenProbPara": 5, "DelProbPara": 3.5, "periodic": True,
+            "samplerMode": "stratified", "seed": seed,
+        },
+    }
+    x32 = x.astype(np.float32)
+    x32[x32 >= np.float32(1.0)] = 0.0  # 1 - tiny rounds to 1 in f32: the same point as 0
+    return SimConfig(config=cfg), x32, w.astype(np.float32)
+
+
 def ring_vorticity(x: np.ndarray, R=0.5, sigma=0.05, gamma=1.0) -> np.ndarray:
     """Gaussian-core vortex ring in the x-y plane about the z axis:
     ω = Γ/(πσ²) exp(-d²/σ²) e_θ with d the distance to the core circle."""

@@ -129,8 +129,13 @@ typedef struct dv_params {
   int32_t kernel_mode;        /* DV_KERNEL_* for VVPE and full BS */
   float blob_delta2;          /* δ² of DV_KERNEL_BLOB3D */
   float blob_coef;            /* f32(V / 4π) of DV_KERNEL_BLOB3D */
-  int32_t compensated;        /* 1: compensated (Neumaier) f32 accumulation in the N-body sums */
-  int32_t reserved[8];
+  int32_t compensated;        /* 1: compensated (Kahan) f32 accumulation in the N-body sums */
+  /* periodic box (new): every axis wraps with period box[d] = domain_end - domain_start;
+   * needs cell_origin_offset = 1, grid_size = box[d] / grid_num[d] on every axis
+   * (cells at least h wide) and grid_num[d] >= 3; distances use the minimum image */
+  int32_t periodic;
+  float box[3];
+  int32_t reserved[4];
 } dv_params;
 
 /* Fields that travel with a particle: dv_grid_build permutes them

@@ -149,7 +149,11 @@ inline int pos_to_index(const dv_params& P, float x, int d) {
   float q = t / P.grid_size;
   if (!(q > -1.0e9f)) q = -1.0e9f;
   if (q > 1.0e9f) q = 1.0e9f;
-  return (int)q;
+  int g = (int)q;
+  // a periodic box holds every position in [start, start + box): a quotient
+  // that rounds up to grid_num belongs to the last cell
+  if (P.periodic) g = g < 0 ? 0 : (g >= P.grid_num[d] ? P.grid_num[d] - 1 : g);
+  return g;
 }
 
 inline int64_t cell_key(const Ctx& c, const int g[3]) {
@@ -177,6 +181,22 @@ inline float transit_weight(const dv_params& P, float x0) {  // dimcv_sph.py:401
   return std::min(std::max(w, 0.0f), 1.0f);
 }
 
+// minimum image on a periodic axis of length L (new option; the reference
+// has no periodic boxes)
+inline float min_image(float d, float L) {
+  const float hl = 0.5f * L;
+  return d > hl ? d - L : (d < -hl ? d + L : d);
+}
+inline V rel(const Ctx& c, V a, V b) {
+  V r{a.x - b.x, a.y - b.y, a.z - b.z};
+  if (c.p.periodic) {
+    r.x = min_image(r.x, c.p.box[0]);
+    r.y = min_image(r.y, c.p.box[1]);
+    if (c.p.dim == 3) r.z = min_image(r.z, c.p.box[2]);
+  }
+  return r;
+}
+
 // for_all_neighbors (particle_system.py:562-586): literal distance test
 template <typename F>
 void for_all_neighbors(const Ctx& c, const float* x, int i, F&& task) {
@@ -189,8 +209,10 @@ void for_all_neighbors(const Ctx& c, const float* x, int i, F&& task) {
       for (int cc = lo2; cc <= hi2; ++cc) {
         int g[3] = {ci[0] + a, ci[1] + b, ci[2] + cc};
         bool ok = true;
-        for (int d = 0; d < P.dim; ++d)
+        for (int d = 0; d < P.dim; ++d) {
+          if (P.periodic) g[d] = g[d] < 0 ? g[d] + P.grid_num[d] : (g[d] >= P.grid_num[d] ? g[d] - P.grid_num[d] : g[d]);
           if (g[d] < 0 || g[d] >= P.grid_num[d]) ok = false;
+        }
         if (!ok) continue;
         int64_t key = cell_key(c, g);
         int s, e;
@@ -208,8 +230,7 @@ void for_all_neighbors(const Ctx& c, const float* x, int i, F&& task) {
         }
         for (int j = s; j < e; ++j) {
           if (j == i) continue;
-          V xj = ldv(c, x, j);
-          V r{xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+          V r = rel(c, xi, ldv(c, x, j));
           if (std::sqrt(norm_sqr(c, r)) < P.support_radius) task(j, r);
         }
       }
@@ -345,7 +366,7 @@ DVO_API int dvo_update_activity(void* h, dv_fields* f) {
   for (int i = range_lo(c); i < range_hi(c); ++i) {
     if (f->material[i] == DV_MATERIAL_SOLID) {
       f->is_active[i] = 1;
-    } else if (f->material[i] == DV_MATERIAL_FLUID) {
+    } else if (f->material[i] == DV_MATERIAL_FLUID && !P.periodic) {
       V x = ldv(*c, f->x, i);
       float xs[3] = {x.x, x.y, x.z};
       for (int j = 0; j < P.dim; ++j)
@@ -498,7 +519,7 @@ DVO_API int dvo_boundary_volume(void* h, dv_fields* f) {
     for_all_neighbors(*c, f->x, i, [&](int j, V) {
       if (f->material[j] == DV_MATERIAL_SOLID) {
         V xj = ldv(*c, f->x, j);
-        V r{xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+        V r = rel(*c, xi, xj);
         delta += cubic_kernel(P, std::sqrt(norm_sqr(*c, r)));
       }
     });
@@ -831,6 +852,17 @@ DVO_API int dvo_advect(void* h, dv_fields* f) {  // dimcv_sph.py:210-218
     }
     V x = ldv(*c, f->x, i);
     x.x += dt * v.x; x.y += dt * v.y; x.z += dt * v.z;
+    if (c->p.periodic) {
+      float* cs[3] = {&x.x, &x.y, &x.z};
+      for (int d = 0; d < c->p.dim; ++d) {
+        if (*cs[d] >= c->p.domain_start[d] + c->p.box[d]) *cs[d] -= c->p.box[d];
+        if (*cs[d] < c->p.domain_start[d]) {
+          *cs[d] += c->p.box[d];
+          // -tiny + box rounds to box: that point is the start of the axis
+          if (*cs[d] >= c->p.domain_start[d] + c->p.box[d]) *cs[d] = c->p.domain_start[d];
+        }
+      }
+    }
     stv(*c, f->x, i, x);
   }
   return 0;
@@ -1088,7 +1120,7 @@ static void vvpe_target(Ctx* c, dv_fields* f, dv_solver_fields* s, int i, bool b
   for (int q = 0; q < c->cnt.num_samples; ++q) {
     int j = s->sample_idx[q];
     V xj = ldv(*c, f->x, j);
-    V r32{xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+    V r32 = rel(*c, xi, xj);
     float rn32 = std::sqrt(norm_sqr(*c, r32));
     if (!(rn32 > P.support_radius)) continue;  // dimcv_sph.py:700
     V w = ld4(s->d_vort_smoothed, j);
@@ -1166,6 +1198,12 @@ DVO_API int dvo_bs_full(void* h, dv_fields* f, const float* omega, const int32_t
       if (j == i) continue;
       V xj = ldv(*c, f->x, j);
       double dx = (double)xi.x - xj.x, dy = (double)xi.y - xj.y, dz = P.dim == 3 ? (double)xi.z - xj.z : 0.0;
+      if (P.periodic) {
+        const double L0 = P.box[0], L1 = P.box[1], L2 = P.box[2];
+        dx = dx > L0 / 2 ? dx - L0 : (dx < -L0 / 2 ? dx + L0 : dx);
+        dy = dy > L1 / 2 ? dy - L1 : (dy < -L1 / 2 ? dy + L1 : dy);
+        if (P.dim == 3) dz = dz > L2 / 2 ? dz - L2 : (dz < -L2 / 2 ? dz + L2 : dz);
+      }
       double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 == 0.0) continue;
       const float* w = omega + 4 * (int64_t)j;

@@ -65,3 +65,29 @@ def test_ring_scene_volume_and_offset():
     # the ring peak vorticity is Γ/(πσ²) on the core circle
     c = np.array([[0.5, 0.0, 0.0]])
     assert abs(np.linalg.norm(scenes.ring_vorticity(c)) - 1.0 / (np.pi * 0.05 ** 2)) < 1e-9
+
+
+def test_periodic_box_grid():
+    cfg, x, w = scenes.periodic2d(65536, seed=0)
+    p = make_params(cfg)
+    # h = 4 r = 2/256; cells of 1/floor(1/h) = 1/128 >= h
+    assert p.periodic == 1 and p.cell_origin_offset == 1 and p.skip_cell0 == 0
+    assert list(p.grid_num)[:2] == [128, 128]
+    assert p.grid_size == np.float32(1.0 / 128) and p.grid_size >= p.support_radius
+    assert list(p.box)[:2] == [1.0, 1.0]
+    assert x.shape == (65536, 2) and x.min() >= 0.0 and x.max() < 1.0
+    vp = 1.25 * 0.8 * (2 * (0.5 / 256)) ** 2
+    assert abs(vp - 1.0 / 65536) < 1e-15
+    # the blobs are periodic: the field at x and x + (1, 0) agree
+    a = scenes.periodic_blobs(np.array([[0.01, 0.3]]), 1)
+    b = scenes.periodic_blobs(np.array([[1.01, 0.3]]), 1)
+    assert abs(a[0] - b[0]) < 1e-12
+
+
+def test_periodic_box_rejects_bad_shapes():
+    from dimcv_sph_b200.config_builder import SimConfig
+    base = {"domainStart": [0.0, 0.0], "domainEnd": [1.0, 0.5], "particleRadius": 0.03,
+            "density0": 1000, "timeStepSize": 1e-3, "gravitation": [0, 0], "periodic": True}
+    # 1/0.12 -> 8 cells of 0.125, 0.5/0.12 -> 4 cells: too few and not the same size
+    with pytest.raises(ValueError):
+        make_params(SimConfig(config={"Configuration": base}))
