@@ -29,6 +29,9 @@ DV_SAMPLE_STRATIFIED = 3
 DV_KERNEL_REF2D = 0
 DV_KERNEL_BLOB3D = 1
 
+DV_VPM_MC = 0
+DV_VPM_FULL = 1
+
 MATERIAL_SOLID = 0
 MATERIAL_FLUID = 1
 
@@ -111,6 +114,16 @@ class DvSolverFields(C.Structure):
         ("v_star", _FP), ("grad_v", _FP), ("d_vort", _FP), ("d_vort_smoothed", _FP),
         ("kvn", _FP), ("kden", _FP), ("x_temp", _FP), ("vorticity_vis", _FP),
         ("v_vort", _FP), ("sample_idx", _IP),
+    ]
+
+
+class DvVpmPlan(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("src_cap", C.c_int32), ("nbr_cap", C.c_int64),
+        ("n_src", C.c_void_p), ("perm", C.c_void_p), ("inv_perm", C.c_void_p),
+        ("nbr_off", C.c_void_p), ("nbr", C.c_void_p), ("src", C.c_void_p), ("src_a", C.c_void_p),
+        ("slot_src", C.c_void_p), ("slot_a", C.c_void_p), ("f", C.c_void_p), ("m_V", C.c_void_p),
+        ("xbar", C.c_void_p),
     ]
 
 

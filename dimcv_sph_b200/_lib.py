@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from ._abi import DvCounters, DvFields, DvParams, DvSolverFields
+from ._abi import DvCounters, DvFields, DvParams, DvSolverFields, DvVpmPlan
 
 LIB_PATH = Path(os.environ.get("DIMCV_LIB", Path(__file__).resolve().parent / "libdimcv.so"))
 
@@ -66,6 +66,12 @@ PROTOTYPES = {
     "dv_fp32_peak": (C.c_int, [_P, C.POINTER(f64)]),
     "dv_density_error_noalloc": (C.c_int, [_PP, _FP, i32, f32, C.POINTER(f64), _P]),
     "dv_profile": (C.c_int, [_P, i32]),
+    "dv_vpm_workspace_bytes": (i64, [_P, i32, i32, i32]),
+    "dv_vpm_plan_build": (C.c_int, [_P, _FP, _SP, i32, C.POINTER(DvVpmPlan)]),
+    "dv_vpm_smooth": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P]),
+    "dv_vpm_smooth_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P]),
+    "dv_vpm_velocity": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, i64]),
+    "dv_vpm_velocity_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P, _P, i64]),
     "dv_profile_read": (C.c_int, [_P, C.POINTER(f64), C.POINTER(i64), C.POINTER(f64)]),
 }
 

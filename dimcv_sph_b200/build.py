@@ -31,6 +31,7 @@ UNITS = {
     "dv_dimcv.cu": ["-fmad=false"],
     "dv_vvpe.cu": [],
     "dv_noalloc.cu": ["-fmad=false"],
+    "dv_vpm.cu": [],
 }
 
 

@@ -360,4 +360,60 @@ DV_API int dv_density_error_noalloc(const dv_params* params, const dv_fields* f,
  * FP32-pipe-bound N-body kernels.  Synchronises. */
 DV_API int dv_fp32_peak(dv_ctx* ctx, double* flops_out);
 
+/* ------------------------------------------------------------------------
+ * Differentiable vortex-particle step (2-D).  No reference counterpart: the
+ * reference has no derivatives.  The step is the SPH vorticity smoothing
+ * (dimcv_sph.py:660-677) followed by the Monte-Carlo Biot-Savart velocity
+ * (dimcv_sph.py:649-719) without the gate, on caller arrays in the sorted
+ * slot order of a plan:
+ *   ω̃_i = m_V_i W(0) ω_i + Σ_{j∈N(i)} m_V_j W(r_ij) ω_j
+ *   u_i = Σ_{j∈N(i)} [c Kε(r_ij) − f_i a_j / r_ij²] ω̃_j r_ij⊥ + f_i Σ_s a_s ω̃_s r_is⊥ / r_is²
+ * (r⊥ = (r_y, −r_x), c = 0.1592 vp_volume, a_s = multiplicity / (kden_s + 1e-8),
+ * f_i = c (S − S_i) / (M − near samples of i)).  A plan freezes neighbour
+ * lists, sources, weights and (with xbar) the periodic images, so the VJPs
+ * are exact derivatives of the frozen step.  Arrays: x [n][2], ω [n],
+ * u [n][2], of the call precision (32: float, 64: double).
+ * ------------------------------------------------------------------------ */
+#define DV_VPM_MC 0   /* sources = the current samples (dv_sample), MC weights */
+#define DV_VPM_FULL 1 /* sources = every particle, a = 1, f = c: full Biot-Savart */
+
+typedef struct dv_vpm_plan {
+  int32_t n;         /* particles = targets, slots [0, n) */
+  int32_t src_cap;   /* capacity of the source arrays (>= M; >= n for DV_VPM_FULL) */
+  int64_t nbr_cap;   /* capacity of nbr */
+  int32_t* n_src;    /* device scalar: number of sources, -1 if the build failed */
+  int32_t* perm;     /* [n] slot -> index of the particle in the caller's order */
+  int32_t* inv_perm; /* [n] caller index -> slot */
+  int32_t* nbr_off;  /* [n+1] CSR offsets */
+  int32_t* nbr;      /* [nbr_cap] neighbour slots, |r| < h */
+  int32_t* src;      /* [src_cap] source slots, ascending */
+  float* src_a;      /* [src_cap] a_s */
+  int32_t* slot_src; /* [n] index in src, or -1 */
+  float* slot_a;     /* [n] a_j (0 where j is no source) */
+  float* f;          /* [n] far factor f_i */
+  float* m_V;        /* [n] volumes */
+  const void* xbar;  /* [n][2] nominal positions fixing the periodic image of every pair,
+                        of the call precision; NULL: minimum image */
+} dv_vpm_plan;
+
+/* Bytes of the caller workspace of dv_vpm_velocity / dv_vpm_velocity_bwd. */
+DV_API int64_t dv_vpm_workspace_bytes(dv_ctx* ctx, int32_t n, int32_t src_cap, int32_t precision);
+/* Fill a plan from the state after dv_grid_build (neighbour lists, sort
+ * permutation) and, for DV_VPM_MC, dv_akde + dv_sample.  Every particle must
+ * be fluid (n == n_fluid).  Asynchronous; *n_src = -1 reports a failed
+ * build (count mismatch, missing lists, capacity). */
+DV_API int dv_vpm_plan_build(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s, int32_t mode,
+                             dv_vpm_plan* plan);
+DV_API int dv_vpm_smooth(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
+                         const void* w, void* w_s);
+/* g_w = (∂ω̃/∂ω)^T g_ws, g_x = (∂ω̃/∂x)^T g_ws (written, not accumulated) */
+DV_API int dv_vpm_smooth_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
+                             const void* w, const void* g_ws, void* g_w, void* g_x);
+DV_API int dv_vpm_velocity(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
+                           const void* w_s, void* u, void* workspace, int64_t workspace_bytes);
+/* g_ws = (∂u/∂ω̃)^T g_u, g_x = (∂u/∂x)^T g_u (written, not accumulated) */
+DV_API int dv_vpm_velocity_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
+                               const void* w_s, const void* g_u, void* g_ws, void* g_x, void* workspace,
+                               int64_t workspace_bytes);
+
 #endif /* DIMCV_H_ */
