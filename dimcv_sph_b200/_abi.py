@@ -89,7 +89,8 @@ class DvParams(C.Structure):
         ("compensated", C.c_int32),
         ("periodic", C.c_int32),
         ("box", F3),
-        ("reserved", C.c_int32 * 4),
+        ("n_scenes", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -125,6 +126,28 @@ class DvVpmPlan(C.Structure):
         ("slot_src", C.c_void_p), ("slot_a", C.c_void_p), ("f", C.c_void_p), ("m_V", C.c_void_p),
         ("xbar", C.c_void_p),
     ]
+
+
+class DvBatchScene(C.Structure):
+    _fields_ = [
+        ("domain_end", F3), ("cap", C.c_int32), ("emit_offset", C.c_int32), ("emit_count", C.c_int32),
+        ("emit_interval", C.c_int32), ("emit_velocity", F3), ("emit_density", C.c_float),
+        ("emit_color", I3), ("emit_volume", C.c_float), ("pad", C.c_int32), ("seed", C.c_uint64),
+    ]
+
+
+class DvSceneState(C.Structure):
+    _fields_ = [
+        ("start", C.c_int32), ("end", C.c_int32), ("n_fluid", C.c_int32), ("n_solid", C.c_int32),
+        ("t_start", C.c_int32), ("n_targets", C.c_int32), ("m_off", C.c_int32), ("num_samples", C.c_int32),
+        ("tile_off", C.c_int32), ("iters_div", C.c_int32), ("iters_p", C.c_int32), ("done", C.c_int32),
+        ("status", C.c_int32), ("emitted", C.c_int32),
+        ("err_div", C.c_double), ("err_p", C.c_double), ("kden_sum", C.c_double),
+        ("kden_sum_f32", C.c_float), ("pad", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
 class DvCounters(C.Structure):

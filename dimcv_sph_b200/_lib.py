@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from ._abi import DvCounters, DvFields, DvParams, DvSolverFields, DvVpmPlan
+from ._abi import DvBatchScene, DvCounters, DvFields, DvParams, DvSceneState, DvSolverFields, DvVpmPlan
 
 LIB_PATH = Path(os.environ.get("DIMCV_LIB", Path(__file__).resolve().parent / "libdimcv.so"))
 
@@ -67,6 +67,11 @@ PROTOTYPES = {
     "dv_density_error_noalloc": (C.c_int, [_PP, _FP, i32, f32, C.POINTER(f64), _P]),
     "dv_profile": (C.c_int, [_P, i32]),
     "dv_vpm_workspace_bytes": (i64, [_P, i32, i32, i32]),
+    "dv_batch_setup": (C.c_int, [_P, C.POINTER(DvBatchScene), i32, _P, i32, f32, i32]),
+    "dv_batch_step": (C.c_int, [_P, _FP, _FP, _SP]),
+    "dv_batch_graph_capture": (C.c_int, [_P, _FP, _FP, _SP, i32]),
+    "dv_batch_graph_launch": (C.c_int, [_P]),
+    "dv_batch_read": (C.c_int, [_P, C.POINTER(DvSceneState), i32, C.POINTER(i64)]),
     "dv_vpm_plan_build": (C.c_int, [_P, _FP, _SP, i32, C.POINTER(DvVpmPlan)]),
     "dv_vpm_smooth": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P]),
     "dv_vpm_smooth_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P]),

@@ -32,6 +32,7 @@ UNITS = {
     "dv_vvpe.cu": [],
     "dv_noalloc.cu": ["-fmad=false"],
     "dv_vpm.cu": [],
+    "dv_batch.cu": ["-fmad=false"],
 }
 
 

@@ -1,0 +1,462 @@
+// Scene batch: S independent scenes stepped together (new: the reference
+// steps one scene per process).  One context holds every scene; a slot's
+// scene id is its object_id, positions are scene-local, and the cell key
+// carries the scene id above the Morton bits, so the sort keeps each scene
+// contiguous and the neighbour sweeps of the single-scene path run on the
+// whole batch without ever crossing scenes.  This unit holds the per-scene
+// pieces: emission on the device, scene ranges and counts after the sort,
+// the per-scene DFSPH convergence test, kden_sum, the sample / target / tile
+// offsets, the step orchestration and its CUDA-graph capture.  Every
+// per-scene reduction is one block per scene summing its slots in a fixed
+// order, so a batch step is deterministic.
+#include <algorithm>
+#include <vector>
+
+#include "dv_internal.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------- emission
+// emit_particle (dimcv_sph.py:616-637) for every scene whose interval
+// divides the step counter: its emitter lattice is appended after the
+// current particles with the fields dv_add_particles writes.
+template <int D>
+__global__ void k_batch_emit(dv_fields F, const dv_batch_scene* __restrict__ sc, int S,
+                             const float* __restrict__ pos, const int64_t* __restrict__ step, dv_counters* C,
+                             int cap, dv_scene_state* st) {
+  extern __shared__ int off[];  // [S + 1]
+  const int64_t t = *step;
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int s = 0; s < S; ++s) {
+      off[s] = o;
+      const int iv = sc[s].emit_interval;
+      if (iv > 0 && sc[s].emit_count > 0 && t % iv == 0) o += sc[s].emit_count;
+    }
+    off[S] = o;
+  }
+  __syncthreads();
+  const int n0 = C->n, total = off[S];
+  const int room = cap - n0 > 0 ? cap - n0 : 0;
+  const int added = total < room ? total : room;
+  for (int k = threadIdx.x; k < added; k += blockDim.x) {
+    int lo = 0, hi = S;  // scene: last s with off[s] <= k
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (off[mid] <= k)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int s = lo - 1;
+    const int e = sc[s].emit_offset + (k - off[s]);
+    const int p = n0 + k;
+    const V3 x{pos[e * D], pos[e * D + 1], D == 3 ? pos[e * D + 2] : 0.0f};
+    const V3 v{sc[s].emit_velocity[0], sc[s].emit_velocity[1], D == 3 ? sc[s].emit_velocity[2] : 0.0f};
+    const float rho = sc[s].emit_density, m_V0 = sc[s].emit_volume;
+    stv<D>(F.x, p, x);
+    stv<D>(F.x0, p, x);
+    stv<D>(F.v, p, v);
+    stv<D>(F.acceleration, p, V3{0.f, 0.f, 0.f});
+    st4(F.vorticity, p, V3{0.f, 0.f, 0.f});
+    F.object_id[p] = s;
+    F.density[p] = rho;
+    F.m_V[p] = m_V0;
+    F.m[p] = m_V0 * rho;  // particle_system.py:325
+    F.pressure[p] = 0.0f;
+    F.material[p] = DV_MATERIAL_FLUID;
+    F.is_dynamic[p] = 1;
+    reinterpret_cast<int4*>(F.color)[p] =
+        make_int4(sc[s].emit_color[0], sc[s].emit_color[1], sc[s].emit_color[2], 0);
+    F.is_active[p] = 1;
+    F.dfsph_factor[p] = 0.0f;
+    F.density_adv[p] = 0.0f;
+    F.is_sample[p] = 0;
+    F.life_time[p] = 0.0f;
+    F.grid_ids[p] = -1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    C->n = n0 + added;
+    C->n_fluid += added;
+    if (added < total) C->status |= DV_WARN_CAPACITY;
+  }
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const int a = min(off[s], added), b = min(off[s + 1], added);
+    st[s].emitted += b - a;
+    if (b - a < off[s + 1] - off[s]) st[s].status |= DV_WARN_CAPACITY;
+  }
+}
+
+// ----------------------------------------------------- ranges and counts
+__global__ void k_batch_clear_ranges(dv_scene_state* st, int S) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < S) {
+    st[s].start = 0;
+    st[s].end = 0;
+  }
+}
+
+// scene ranges from the sorted keys (scene id above `shift` bits)
+__global__ void k_batch_ranges(const uint32_t* __restrict__ keys, const dv_counters* __restrict__ C, int shift,
+                               int S, dv_scene_state* st) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = C->n;
+  if (p >= n) return;
+  const int s = (int)(keys[p] >> shift);
+  if (s < 0 || s >= S) return;
+  if (p == 0 || (int)(keys[p - 1] >> shift) != s) st[s].start = p;
+  if (p == n - 1 || (int)(keys[p + 1] >> shift) != s) st[s].end = p + 1;
+}
+
+// fluid / solid / target counts per scene (one block per scene)
+template <int D>
+__global__ void k_batch_counts(dv_params P, dv_fields F, dv_scene_state* st) {
+  const int s = blockIdx.x;
+  const int a = st[s].start, b = st[s].end;
+  int fl = 0, so = 0, tg = 0;
+  for (int i = a + threadIdx.x; i < b; i += blockDim.x) {
+    const int m = F.material[i];
+    fl += m == DV_MATERIAL_FLUID;
+    so += m == DV_MATERIAL_SOLID;
+    tg += m == DV_MATERIAL_FLUID && in_vortex_domain<D>(P, ldv<D>(F.x, i));
+  }
+  fl = block_sum<int>(fl);
+  so = block_sum<int>(so);
+  tg = block_sum<int>(tg);
+  if (threadIdx.x == 0) {
+    st[s].n_fluid = fl;
+    st[s].n_solid = so;
+    st[s].n_targets = tg;
+  }
+}
+
+// kden_sum of every scene (compute_kernel_density, dimcv_sph.py:738-751):
+// FP64 over the scene's targets, in slot order
+template <int D>
+__global__ void k_batch_kden(dv_params P, dv_fields F, const float* __restrict__ kden, dv_scene_state* st) {
+  const int s = blockIdx.x;
+  const int a = st[s].start, b = st[s].end;
+  double acc = 0.0;
+  for (int i = a + threadIdx.x; i < b; i += blockDim.x)
+    if (F.material[i] == DV_MATERIAL_FLUID && in_vortex_domain<D>(P, ldv<D>(F.x, i))) acc += (double)kden[i];
+  acc = block_sum<double>(acc);
+  if (threadIdx.x == 0) {
+    st[s].kden_sum = acc;
+    st[s].kden_sum_f32 = (float)acc;
+  }
+}
+
+// target, sample and far-field tile offsets; M_s = max(1, floor(frac · fluid_s))
+// where the scene has targets with a positive kden_sum, else 0 (dv_sample)
+__global__ void k_batch_offsets(dv_scene_state* st, int S, float frac, int tile_w, dv_counters* C,
+                                int32_t* misc) {
+  int t = 0, m = 0, tiles = 0;
+  for (int s = 0; s < S; ++s) {
+    st[s].t_start = t;
+    st[s].m_off = m;
+    st[s].tile_off = tiles;
+    const int nt = st[s].n_targets;
+    int M = 0;
+    if (nt > 0 && st[s].kden_sum > 0.0) {
+      M = (int)((double)frac * (double)st[s].n_fluid);
+      if (M < 1) M = 1;
+    }
+    st[s].num_samples = M;
+    t += nt;
+    m += M;
+    tiles += (nt + tile_w - 1) / tile_w;
+  }
+  C->num_samples = m;
+  misc[0] = tiles;
+}
+
+// ----------------------------------------------------------- DFSPH solves
+__global__ void k_batch_solve_reset(dv_scene_state* st, int32_t* done, int S, int which) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < S) {
+    done[s] = 0;
+    if (which == 0)
+      st[s].iters_div = 0;
+    else
+      st[s].iters_p = 0;
+  }
+  if (s == 0) done[S] = 0;
+}
+
+// k_solve_finalize per scene: FP64 sum of the scene's residual terms, average
+// over its fluid count, convergence test against eta or the iteration cap
+__global__ void k_batch_solve_finalize(const double* __restrict__ err, dv_scene_state* st, int32_t* done,
+                                       double eta, int max_iter, int which) {
+  const int s = blockIdx.x;
+  if (done[s]) return;
+  const int a = st[s].start, b = st[s].end;
+  double acc = 0.0;
+  for (int i = a + threadIdx.x; i < b; i += blockDim.x) acc += err[i];
+  acc = block_sum<double>(acc);
+  if (threadIdx.x == 0) {
+    const int nf = st[s].n_fluid;
+    const double avg = nf > 0 ? acc / (double)nf : 0.0;
+    const int it = which == 0 ? ++st[s].iters_div : ++st[s].iters_p;
+    if (which == 0)
+      st[s].err_div = avg;
+    else
+      st[s].err_p = avg;
+    if (!isfinite(avg)) st[s].status |= DV_WARN_NAN;
+    if (avg <= eta || nf == 0) {
+      done[s] = 1;
+    } else if (it >= max_iter) {
+      done[s] = 1;
+      st[s].status |= which == 0 ? DV_WARN_DIV_NOT_CONVERGED : DV_WARN_P_NOT_CONVERGED;
+    }
+  }
+}
+
+__global__ void k_batch_all_done(int32_t* done, int S) {
+  int all = 1;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) all &= done[s] != 0;
+  all = block_sum<int>(all);
+  if (threadIdx.x == 0) done[S] = all == (int)blockDim.x ? 1 : 0;  // threads without a scene count 1
+}
+
+__global__ void k_batch_step_inc(int64_t* step) { *step += 1; }
+
+int check_batch(dv_ctx* c) {
+  if (!c) return DV_EINVAL;
+  if (!c->batch) return dv_fail(c, DV_EINVAL, "the context has no scene batch (dv_batch_setup)");
+  return DV_OK;
+}
+
+}  // namespace
+
+int dv_batch_solve_reset(dv_ctx* c, int which) {
+  dv_batch_state* b = c->batch;
+  k_batch_solve_reset<<<dv_blocks(b->S), DV_THREADS, 0, c->stream>>>(b->d_state, b->d_done, b->S, which);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+int dv_batch_solve_finalize(dv_ctx* c, int which) {
+  dv_batch_state* b = c->batch;
+  const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
+  const double eta = which == 0 ? c->p.eta_div : c->p.eta_p;
+  k_batch_solve_finalize<<<b->S, DV_THREADS, 0, c->stream>>>(b->d_err, b->d_state, b->d_done, eta, max_iter,
+                                                              which);
+  DV_LAUNCHED(c);
+  k_batch_all_done<<<1, 1024, 0, c->stream>>>(b->d_done, b->S);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_scenes, const float* emit_pos,
+                          int32_t n_emit, float mc_fraction, int32_t sample_mode) {
+  if (!c || !scenes || n_scenes < 1) return DV_EINVAL;
+  if (sample_mode != DV_SAMPLE_INVERSE_CDF && sample_mode != DV_SAMPLE_STRATIFIED)
+    return dv_fail(c, DV_EINVAL, "dv_batch_setup: sample_mode must be inverse-CDF or stratified");
+  if (c->p.n_scenes != n_scenes)
+    return dv_fail(c, DV_EINVAL, "dv_batch_setup: %d scenes, the context was created for %d", n_scenes,
+                   c->p.n_scenes);
+  if (c->p.periodic) return dv_fail(c, DV_EUNSUPPORTED, "scene batches of periodic boxes are not built");
+  if (n_emit < 0 || (n_emit > 0 && !emit_pos)) return dv_fail(c, DV_EINVAL, "dv_batch_setup: emitter arrays");
+  if (n_scenes > 4096) return dv_fail(c, DV_EINVAL, "dv_batch_setup: at most 4096 scenes");
+  int64_t cap_sum = 0;
+  for (int s = 0; s < n_scenes; ++s) {
+    const dv_batch_scene& q = scenes[s];
+    if (q.cap < 0 || q.emit_count < 0 || q.emit_offset < 0 || q.emit_offset + q.emit_count > n_emit ||
+        q.emit_interval < 0)
+      return dv_fail(c, DV_EINVAL, "dv_batch_setup: scene %d has an invalid emitter or capacity", s);
+    cap_sum += q.cap;
+  }
+  (void)cap_sum;
+  if (c->batch) return dv_fail(c, DV_EINVAL, "dv_batch_setup: already set up");
+  dv_batch_state* b = new dv_batch_state();
+  b->S = n_scenes;
+  b->mc_fraction = mc_fraction;
+  b->stratified = sample_mode == DV_SAMPLE_STRATIFIED;
+  b->n_emit = n_emit;
+  // far-field tiles are at least 512 targets wide: sum_s ceil(n_s / 512) <= cap / 512 + S
+  b->cap_tiles = c->cap / 512 + n_scenes + 2;
+  b->m_cap = c->cap;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes < 1 ? 1 : bytes);
+  };
+  al((void**)&b->d_scenes, sizeof(dv_batch_scene) * n_scenes);
+  al((void**)&b->d_state, sizeof(dv_scene_state) * n_scenes);
+  al((void**)&b->d_done, sizeof(int32_t) * (n_scenes + 1));
+  al((void**)&b->d_misc, sizeof(int32_t) * 4);
+  al((void**)&b->d_err, sizeof(double) * c->cap);
+  al((void**)&b->d_step, sizeof(int64_t));
+  al((void**)&b->d_emit, sizeof(float) * c->p.dim * std::max(n_emit, 1));
+  al((void**)&c->d_scene_end, sizeof(float) * 3 * n_scenes);
+  std::vector<float> ends(3 * n_scenes);
+  for (int s = 0; s < n_scenes; ++s)
+    for (int d = 0; d < 3; ++d) ends[3 * s + d] = scenes[s].domain_end[d];
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_scenes, scenes, sizeof(dv_batch_scene) * n_scenes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->d_state, 0, sizeof(dv_scene_state) * n_scenes);
+  if (e == cudaSuccess) e = cudaMemset(b->d_done, 0, sizeof(int32_t) * (n_scenes + 1));
+  if (e == cudaSuccess) e = cudaMemset(b->d_misc, 0, sizeof(int32_t) * 4);
+  if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(double) * c->cap);
+  if (e == cudaSuccess) e = cudaMemset(b->d_step, 0, sizeof(int64_t));
+  if (e == cudaSuccess && n_emit > 0)
+    e = cudaMemcpy(b->d_emit, emit_pos, sizeof(float) * c->p.dim * n_emit, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_scene_end, ends.data(), sizeof(float) * 3 * n_scenes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->gstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev0, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev1, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  c->batch = b;  // freed by dv_destroy even on failure
+  if (e != cudaSuccess) return dv_cuda_check(c, e, "dv_batch_setup");
+  c->n_upper = c->cap;  // static launch shapes
+  return DV_OK;
+}
+
+void dv_batch_free(dv_ctx* c) {
+  dv_batch_state* b = c->batch;
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->gstream) cudaStreamDestroy(b->gstream);
+  cudaFree(b->d_scenes);
+  cudaFree(b->d_state);
+  cudaFree(b->d_done);
+  cudaFree(b->d_misc);
+  cudaFree(b->d_err);
+  cudaFree(b->d_step);
+  cudaFree(b->d_emit);
+  cudaFree(c->d_scene_end);
+  c->d_scene_end = nullptr;
+  delete b;
+  c->batch = nullptr;
+}
+
+#define DV_TRY(call)         \
+  do {                       \
+    int rc_ = (call);        \
+    if (rc_) return rc_;     \
+  } while (0)
+
+DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, const dv_solver_fields* s) {
+  DV_TRY(check_batch(c));
+  if (!src || !dst || !s) return DV_EINVAL;
+  dv_batch_state* b = c->batch;
+  const int S = b->S;
+  // emission + activity on the current set, grid build into the other
+  if (c->p.dim == 2)
+    k_batch_emit<2><<<1, 1024, sizeof(int) * (S + 1), c->stream>>>(*src, b->d_scenes, S, b->d_emit, b->d_step,
+                                                                   c->d_cnt, (int)c->cap, b->d_state);
+  else
+    k_batch_emit<3><<<1, 1024, sizeof(int) * (S + 1), c->stream>>>(*src, b->d_scenes, S, b->d_emit, b->d_step,
+                                                                   c->d_cnt, (int)c->cap, b->d_state);
+  DV_LAUNCHED(c);
+  DV_TRY(dv_invalidate_lists(c));
+  DV_TRY(dv_update_activity(c, src));
+  DV_TRY(dv_grid_build(c, src, dst));
+  k_batch_clear_ranges<<<dv_blocks(S), DV_THREADS, 0, c->stream>>>(b->d_state, S);
+  DV_LAUNCHED(c);
+  k_batch_ranges<<<dv_blocks(c->cap), DV_THREADS, 0, c->stream>>>(c->keys[c->perm_buf], c->d_cnt, c->scene_shift,
+                                                                  S, b->d_state);
+  DV_LAUNCHED(c);
+  if (c->p.dim == 2)
+    k_batch_counts<2><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, b->d_state);
+  else
+    k_batch_counts<3><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, b->d_state);
+  DV_LAUNCHED(c);
+  // substep (karman_vortex.py:232-242)
+  DV_TRY(dv_densities(c, dst));
+  DV_TRY(dv_dfsph_factor(c, dst));
+  DV_TRY(dv_density_change(c, dst));
+  DV_TRY(dv_scale_factor(c, dst, c->p.inv_dt));
+  DV_TRY(dv_batch_solve(c, dst, 0));
+  DV_TRY(dv_scale_factor(c, dst, c->p.dt));
+  DV_TRY(dv_nonpressure(c, dst));
+  DV_TRY(dv_dimcv_vorticity(c, dst, s));
+  DV_TRY(dv_d_vorticity(c, dst, s));
+  DV_TRY(dv_smooth_d_vort(c, dst, s));
+  DV_TRY(dv_kvn_sample(c, dst, s, 0, 0, 0));
+  DV_TRY(dv_akde(c, dst, s));
+  if (c->p.dim == 2)
+    k_batch_kden<2><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
+  else
+    k_batch_kden<3><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
+  DV_LAUNCHED(c);
+  k_batch_offsets<<<1, 1, 0, c->stream>>>(b->d_state, S, b->mc_fraction, dv_far_tile_width(c), c->d_cnt,
+                                          b->d_misc);
+  DV_LAUNCHED(c);
+  DV_TRY(dv_build_targets(c, dst));
+  DV_TRY(dv_batch_draw(c, s));
+  DV_TRY(dv_batch_vvpe(c, dst, s));
+  DV_TRY(dv_life_time(c, dst));
+  DV_TRY(dv_predict_velocity(c, dst));
+  DV_TRY(dv_density_adv(c, dst));
+  DV_TRY(dv_scale_factor(c, dst, c->p.inv_dt2));
+  DV_TRY(dv_batch_solve(c, dst, 1));
+  DV_TRY(dv_advect(c, dst));
+  k_batch_step_inc<<<1, 1, 0, c->stream>>>(b->d_step);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+DV_API int dv_batch_graph_capture(dv_ctx* c, const dv_fields* a, const dv_fields* bf, const dv_solver_fields* s,
+                                  int32_t steps) {
+  DV_TRY(check_batch(c));
+  if (!a || !bf || !s || steps < 2 || steps % 2) return dv_fail(c, DV_EINVAL, "dv_batch_graph_capture: need an even step count >= 2");
+  dv_batch_state* b = c->batch;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  // capture on the context's own non-blocking stream (a legacy default stream cannot be captured)
+  cudaStream_t saved = c->stream;
+  DV_CK(c, cudaEventRecord(b->ev0, saved));
+  DV_CK(c, cudaStreamWaitEvent(b->gstream, b->ev0, 0));
+  c->stream = b->gstream;
+  b->capturing = true;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(b->gstream, cudaStreamCaptureModeThreadLocal);
+  int rc = DV_OK;
+  if (e == cudaSuccess) {
+    for (int k = 0; k < steps && rc == DV_OK; ++k) rc = dv_batch_step(c, k % 2 ? bf : a, k % 2 ? a : bf, s);
+    e = cudaStreamEndCapture(b->gstream, &g);
+  }
+  b->capturing = false;
+  c->stream = saved;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return dv_cuda_check(c, e, "dv_batch_graph_capture");
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return dv_cuda_check(c, e, "cudaGraphInstantiate");
+  return DV_OK;
+}
+
+DV_API int dv_batch_graph_launch(dv_ctx* c) {
+  DV_TRY(check_batch(c));
+  dv_batch_state* b = c->batch;
+  if (!b->graph) return dv_fail(c, DV_EINVAL, "dv_batch_graph_launch: no captured graph");
+  DV_CK(c, cudaEventRecord(b->ev0, c->stream));
+  DV_CK(c, cudaStreamWaitEvent(b->gstream, b->ev0, 0));
+  DV_CK(c, cudaGraphLaunch(b->graph, b->gstream));
+  DV_CK(c, cudaEventRecord(b->ev1, b->gstream));
+  DV_CK(c, cudaStreamWaitEvent(c->stream, b->ev1, 0));
+  c->launches++;
+  return DV_OK;
+}
+
+DV_API int dv_batch_read(dv_ctx* c, dv_scene_state* out, int32_t n_scenes, int64_t* step) {
+  DV_TRY(check_batch(c));
+  dv_batch_state* b = c->batch;
+  if (out && n_scenes > 0) {
+    DV_CK(c, cudaMemcpyAsync(out, b->d_state, sizeof(dv_scene_state) * std::min(n_scenes, b->S),
+                             cudaMemcpyDeviceToHost, c->stream));
+  }
+  int64_t st = 0;
+  DV_CK(c, cudaMemcpyAsync(&st, b->d_step, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  DV_CK(c, cudaStreamSynchronize(c->stream));
+  if (step) *step = st;
+  return DV_OK;
+}

@@ -74,6 +74,15 @@ static int build_morton(dv_ctx* c) {
       if (l < bits[d]) pos[d][l] = next++;
   c->ncells = (int64_t)1 << total;
   c->kbits = total + 1;
+  if (P.n_scenes > 1) {  // scene id above the Morton bits
+    int sbits = 0;
+    while ((1 << sbits) < P.n_scenes) ++sbits;
+    if (total + sbits > 30)
+      return dv_fail(c, DV_EUNSUPPORTED, "scene batch needs %d key bits (max 30)", total + sbits);
+    c->scene_shift = total;
+    c->ncells = (int64_t)1 << (total + sbits);
+    c->kbits = total + sbits + 1;
+  }
   c->npasses = (c->kbits + 7) / 8;
   for (int d = 0; d < 3; ++d) {
     int g = d < P.dim ? P.grid_num[d] : 1;
@@ -100,6 +109,7 @@ static cudaError_t alloc(T** p, int64_t count) {
 
 DV_API void dv_destroy(dv_ctx* c) {
   if (!c) return;
+  dv_batch_free(c);
   void* ptrs[] = {c->d_cnt,   c->d_flag,    c->keys[0],   c->keys[1],   c->vals[0], c->vals[1],
                   c->hist,    c->cell_start, c->cell_end, c->mt[0],     c->mt[1],   c->mt[2],
                   c->scan_part, c->dscan_part, c->red_part, c->ired_part, c->flags, c->offs,
@@ -217,7 +227,7 @@ DV_API int dv_get_counters(dv_ctx* c, dv_counters* out) {
   DV_CK(c, cudaMemcpyAsync(c->h_cnt, c->d_cnt, sizeof(dv_counters), cudaMemcpyDeviceToHost, c->stream));
   DV_CK(c, cudaStreamSynchronize(c->stream));
   *out = *c->h_cnt;
-  c->n_upper = out->n;
+  c->n_upper = c->batch ? c->cap : out->n;  // a scene batch keeps capacity-sized launch shapes
   return DV_OK;
 }
 
@@ -234,7 +244,7 @@ DV_API int dv_set_counts(dv_ctx* c, int32_t n, int32_t n_fluid, int32_t n_solid)
                    n, n_fluid, n_solid, (long long)c->cap);
   k_set_counts<<<1, 1, 0, c->stream>>>(c->d_cnt, n, n_fluid, n_solid);
   DV_LAUNCHED(c);
-  c->n_upper = n;
+  c->n_upper = c->batch ? c->cap : n;
   return dv_invalidate_lists(c);
 }
 

@@ -305,6 +305,64 @@ __global__ void k_cdf_draw(const double* __restrict__ cdf_ex, const int32_t* __r
 
 __global__ void k_set_num_samples(dv_counters* C, int M) { C->num_samples = M; }
 
+// Scene batch: draw t belongs to the scene s with m_off_s <= t < m_off_s + M_s;
+// with local index k = t - m_off_s it is k_cdf_draw of that scene alone
+// (Philox keyed by (k, 2, step, seed_s); stratified: u = (k + ξ)/M_s) through
+// the scene's segment [t_start_s, t_start_s + n_targets_s) of the batch CDF.
+__global__ void k_batch_draw(const double* __restrict__ cdf_ex, const int32_t* __restrict__ targets,
+                             const float* __restrict__ kden, const dv_scene_state* __restrict__ st,
+                             const dv_batch_scene* __restrict__ sc, int S, const int64_t* __restrict__ step,
+                             const dv_counters* __restrict__ C, int stratified, int32_t* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C->num_samples) return;
+  int lo = 0, hi = S;  // last s with m_off_s <= t
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (st[mid].m_off <= t)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  const int s = lo - 1;
+  const int k = t - st[s].m_off, M = st[s].num_samples;
+  const int a = st[s].t_start, nt = st[s].n_targets;
+  const uint64_t seed = sc[s].seed, stp = (uint64_t)*step;
+  DvRand4 rnd = dv_philox((uint32_t)k, 2u, (uint32_t)stp, (uint32_t)(stp >> 32), (uint32_t)seed,
+                          (uint32_t)(seed >> 32));
+  double u = dv_u01d(rnd.v[0], rnd.v[1]);
+  if (stratified) u = ((double)k + u) / (double)M;
+  const double base = cdf_ex[a];
+  const double total = cdf_ex[a + nt - 1] + (double)kden[targets[a + nt - 1]] - base;
+  const double y = base + u * total;
+  int l = a, h = a + nt;  // upper_bound in the scene's segment
+  while (l < h) {
+    const int mid = (l + h) >> 1;
+    if (cdf_ex[mid] <= y)
+      l = mid + 1;
+    else
+      h = mid;
+  }
+  int q = l - 1;
+  if (q < a) q = a;
+  while (q > a && !(kden[targets[q]] > 0.0f)) --q;
+  out[t] = targets[q];
+}
+
+int dv_batch_draw(dv_ctx* c, const dv_solver_fields* s) {
+  dv_batch_state* b = c->batch;
+  const int m = (int)std::min<int64_t>(c->n_upper, c->cap);
+  k_cdf_weights<<<dv_blocks(m), DV_THREADS, 0, c->stream>>>(c->targets, s->kden, c->d_cnt, m,
+                                                          reinterpret_cast<double*>(c->near_v));
+  DV_LAUNCHED(c);
+  int rc = dv_scan_f64(c, reinterpret_cast<double*>(c->near_v), c->cdf, m);
+  if (rc) return rc;
+  k_batch_draw<<<dv_blocks(b->m_cap), DV_THREADS, 0, c->stream>>>(c->cdf, c->targets, s->kden, b->d_state,
+                                                                  b->d_scenes, b->S, b->d_step, c->d_cnt,
+                                                                  b->stratified, s->sample_idx);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
 // --------------------------------------------------------- VVPE near field
 // vort2vel_neighbors_2d_task (dimcv_sph.py:649-658) for each target:
 // near_v = 0.1592 V Σ_fluid Kε(|r_xy|) (r_xy × ω̃_j) and

@@ -12,8 +12,11 @@
 // update_activity (particle_system.py:413-427): solids are forced active,
 // fluid outside [domain_start, domain_end] (strict) becomes inactive.  The
 // fluid count is recomputed from the compaction (dv_grid_build).
+// In a scene batch (scene_end != NULL) the box of slot i ends at
+// scene_end[3 * object_id[i]].
 template <int D>
-__global__ void k_update_activity(dv_params P, dv_fields F, const dv_counters* __restrict__ C) {
+__global__ void k_update_activity(dv_params P, dv_fields F, const dv_counters* __restrict__ C,
+                                  const float* __restrict__ scene_end) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= C->n) return;
   int mat = F.material[i];
@@ -21,9 +24,16 @@ __global__ void k_update_activity(dv_params P, dv_fields F, const dv_counters* _
     F.is_active[i] = 1;
   } else if (mat == DV_MATERIAL_FLUID && !P.periodic) {  // nothing leaves a periodic box
     V3 x = ldv<D>(F.x, i);
-    bool out = x.x < P.domain_start[0] || x.x > P.domain_end[0] || x.y < P.domain_start[1] ||
-               x.y > P.domain_end[1];
-    if (D == 3) out = out || x.z < P.domain_start[2] || x.z > P.domain_end[2];
+    float e0 = P.domain_end[0], e1 = P.domain_end[1], e2 = P.domain_end[2];
+    if (scene_end) {
+      const int s = F.object_id[i];
+      if (s < 0 || s >= P.n_scenes) return;
+      e0 = scene_end[3 * s];
+      e1 = scene_end[3 * s + 1];
+      e2 = scene_end[3 * s + 2];
+    }
+    bool out = x.x < P.domain_start[0] || x.x > e0 || x.y < P.domain_start[1] || x.y > e1;
+    if (D == 3) out = out || x.z < P.domain_start[2] || x.z > e2;
     if (out) F.is_active[i] = 0;
   }
 }
@@ -31,10 +41,12 @@ __global__ void k_update_activity(dv_params P, dv_fields F, const dv_counters* _
 DV_API int dv_update_activity(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   int nb = dv_blocks(c->n_upper);
+  const float* se = c->p.n_scenes > 1 ? c->d_scene_end : nullptr;
+  if (c->p.n_scenes > 1 && !se) return dv_fail(c, DV_EINVAL, "scene batch without scene table");
   if (c->p.dim == 2)
-    k_update_activity<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *f, c->d_cnt);
+    k_update_activity<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *f, c->d_cnt, se);
   else
-    k_update_activity<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *f, c->d_cnt);
+    k_update_activity<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *f, c->d_cnt, se);
   DV_LAUNCHED(c);
   return DV_OK;
 }
@@ -45,7 +57,7 @@ DV_API int dv_update_activity(dv_ctx* c, const dv_fields* f) {
 // particle_partition, which is order-preserving, into the stable sort).
 template <int D>
 __global__ void k_cell_keys(dv_params P, dv_fields F, DevGrid G, dv_counters* C, uint32_t* keys,
-                            uint32_t invalid) {
+                            uint32_t invalid, const int32_t* __restrict__ scene, int shift) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int n = C->n;
   if (i >= n) return;
@@ -64,6 +76,7 @@ __global__ void k_cell_keys(dv_params P, dv_fields F, DevGrid G, dv_counters* C,
     }
     key = G.mt0[c0] | G.mt1[c1];
     if (D == 3) key |= G.mt2[c2];
+    if (scene) key |= (uint32_t)scene[i] << shift;  // scene batch: scene-major cell order
   }
   keys[i] = key;
 }
@@ -335,10 +348,14 @@ DV_API int dv_grid_build(dv_ctx* c, const dv_fields* src, const dv_fields* dst) 
   rc = dv_invalidate_lists(c);
   if (rc) return rc;
   DevGrid G = dv_grid_cells(c);
+  const bool batch = c->p.n_scenes > 1;
+  const int32_t* scn = batch ? src->object_id : nullptr;
   if (c->p.dim == 2)
-    k_cell_keys<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *src, G, c->d_cnt, c->keys[0], invalid);
+    k_cell_keys<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *src, G, c->d_cnt, c->keys[0], invalid, scn,
+                                                     c->scene_shift);
   else
-    k_cell_keys<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *src, G, c->d_cnt, c->keys[0], invalid);
+    k_cell_keys<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, *src, G, c->d_cnt, c->keys[0], invalid, scn,
+                                                     c->scene_shift);
   DV_LAUNCHED(c);
   // radix passes
   const int ntiles = (int)std::max<int64_t>(1, (nu + RS_TILE - 1) / RS_TILE);
@@ -373,6 +390,7 @@ DV_API int dv_grid_build(dv_ctx* c, const dv_fields* src, const dv_fields* dst) 
   DV_LAUNCHED(c);
   k_finalize_counts<<<1, 1024, 0, c->stream>>>(c->ired_part, nb, c->d_flag + 1, c->d_cnt);
   DV_LAUNCHED(c);
+  c->scene_ptr = batch ? dst->object_id : nullptr;  // scene of each sorted slot
   return build_csr(c, dst);
 }
 

@@ -73,6 +73,14 @@ struct dv_ctx {
   int64_t nbr_cap = 0;
   int32_t* d_nbr_ok = nullptr;  // 1 while the lists match the current positions
 
+  // scene batch (n_scenes > 1): cell keys carry the scene id above
+  // scene_shift bits; scene_ptr is the scene id of each slot of the sorted
+  // set (its object_id array); scene_end is [n_scenes][3] per-scene domain ends
+  int scene_shift = 0;
+  const int32_t* scene_ptr = nullptr;
+  float* d_scene_end = nullptr;
+  struct dv_batch_state* batch = nullptr;
+
   // far-field kernel profiling (dv_profile)
   bool prof = false;
   static constexpr int kProfPool = 512;
@@ -114,15 +122,53 @@ struct DevGrid {
   const uint32_t* noff;
   const int32_t* nidx;
   const int32_t* nok;
+  // scene batch: the cell key of slot i is (scene[i] << scene_shift) | Morton
+  const int32_t* scene;
+  int scene_shift;
 };
 static inline DevGrid dv_grid(const dv_ctx* c) {
   return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2], c->nbr_off, c->nbr_idx,
-                 c->d_nbr_ok};
+                 c->d_nbr_ok, c->scene_ptr, c->scene_shift};
 }
 // the cell-scan form only (used to build the neighbour lists)
 static inline DevGrid dv_grid_cells(const dv_ctx* c) {
-  return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2], nullptr, nullptr, nullptr};
+  return DevGrid{c->cell_start, c->cell_end, c->mt[0], c->mt[1], c->mt[2], nullptr, nullptr, nullptr,
+                 c->scene_ptr, c->scene_shift};
 }
+
+// ------------------------------------------------------------- scene batch
+// Host-side state of a scene batch (dv_batch_setup); every pointer is device.
+struct dv_batch_state {
+  int S = 0;
+  float mc_fraction = 0.0625f;
+  dv_batch_scene* d_scenes = nullptr; // [S]
+  dv_scene_state* d_state = nullptr;  // [S]
+  int32_t* d_done = nullptr;          // [S + 1]: per-scene solve done; [S]: every scene done
+  int32_t* d_misc = nullptr;          // [0]: far-field tiles this step
+  double* d_err = nullptr;            // [cap] per-slot residual terms of the solves
+  int64_t* d_step = nullptr;          // step counter (emission schedule, sampler stream)
+  float* d_emit = nullptr;            // [n_emit][dim]
+  int32_t n_emit = 0;
+  int64_t cap_tiles = 0;              // launch bound of the far-field work list
+  int64_t m_cap = 0;                  // launch bound of the total sample count
+  bool capturing = false;             // unroll the Jacobi loops (no host polling)
+  int stratified = 0;                 // DV_SAMPLE_STRATIFIED draws, else i.i.d.
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+// dv_batch.cu
+void dv_batch_free(dv_ctx* c);
+int dv_batch_solve_reset(dv_ctx* c, int which);
+int dv_batch_solve_finalize(dv_ctx* c, int which);
+// dv_sph.cu: one DFSPH Jacobi solve with per-scene convergence
+int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which);
+// dv_dimcv.cu: per-scene inverse-CDF draws (targets built)
+int dv_batch_draw(dv_ctx* c, const dv_solver_fields* s);
+// dv_vvpe.cu: near field, far field (scene targets x scene samples), gate
+int dv_batch_vvpe(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s);
+int dv_far_tile_width(const dv_ctx* c);
+int dv_build_targets(dv_ctx* c, const dv_fields* f);
 
 // ------------------------------------------------------------- scan helpers
 // Exclusive scan of uint32 / double arrays on the context stream
@@ -307,6 +353,7 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
   int c0 = cell_coord(P, xi.x, 0), c1 = cell_coord(P, xi.y, 1);
   int c2 = D == 3 ? cell_coord(P, xi.z, 2) : 0;
   const float lim = P.nbr_r2_limit;
+  const uint32_t sk = G.scene ? ((uint32_t)__ldg(G.scene + i) << G.scene_shift) : 0u;
 #pragma unroll 1
   for (int a = -1; a <= 1; ++a) {
     int gx = cell_step(P, c0, a, P.grid_num[0]);
@@ -325,7 +372,8 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
           if (gz < 0) continue;
           key |= __ldg(G.mt2 + gz);
         }
-        if (P.skip_cell0 && key == 0u) continue;
+        if (P.skip_cell0 && key == 0u) continue;  // the scene's own flat cell 0
+        key |= sk;
         int s = __ldg(G.start + key), e = __ldg(G.end + key);
 #pragma unroll 1
         for (int j = s; j < e; ++j) {

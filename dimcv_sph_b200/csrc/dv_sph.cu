@@ -85,13 +85,19 @@ __global__ void k_scale_factor(dv_fields F, float s, const dv_counters* __restri
 // ------------------------------------------------------- density change
 // compute_density_change (dimcv_sph.py:337-374); optionally the block
 // partial of compute_density_error(0) (dimcv_sph.py:407-419) in FP64.
+//
+// Scene batch (scene != NULL): done[] is per scene (the slot's scene id),
+// converged scenes are skipped per thread, and the error term of every slot
+// goes to err_out[i] (0 where none) for the per-scene sums.
 template <int D>
 __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                 const int32_t* __restrict__ done, double* __restrict__ part) {
-  if (done && *done) return;
+                                 const int32_t* __restrict__ done, double* __restrict__ part,
+                                 const int32_t* __restrict__ scene, double* __restrict__ err_out) {
+  if (done && (scene ? done[P.n_scenes] : *done)) return;  // [n_scenes]: every scene converged
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
-  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+  const bool live = i < C->n && !(scene && done && done[scene[i]]);
+  if (live && F.material[i] == DV_MATERIAL_FLUID) {
     V3 xi = ldv<D>(F.x, i);
     V3 vi = ldv<D>(F.v, i);
     float adv = 0.0f;
@@ -108,12 +114,14 @@ __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_c
     float da = fmaxf(adv, 0.0f);
     if (nn < P.neighbor_min) da = 0.0f;
     F.density_adv[i] = da;
-    if (part) {
+    if (part || err_out) {
       float term = P.has_transit ? transit_weight(P, xi.x) * (da - 0.0f) : (da - 0.0f);
       err = (double)term;
     }
   }
-  if (part) {
+  if (err_out) {
+    if (live) err_out[i] = err;
+  } else if (part) {
     double s = block_sum<double>(err);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
   }
@@ -124,11 +132,13 @@ __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_c
 // compute_density_error(density0).
 template <int D>
 __global__ void k_density_adv(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                              const int32_t* __restrict__ done, double* __restrict__ part) {
-  if (done && *done) return;
+                              const int32_t* __restrict__ done, double* __restrict__ part,
+                              const int32_t* __restrict__ scene, double* __restrict__ err_out) {
+  if (done && (scene ? done[P.n_scenes] : *done)) return;  // [n_scenes]: every scene converged
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
-  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+  const bool live = i < C->n && !(scene && done && done[scene[i]]);
+  if (live && F.material[i] == DV_MATERIAL_FLUID) {
     V3 xi = ldv<D>(F.x, i);
     V3 vi = ldv<D>(F.v, i);
     float delta = 0.0f;
@@ -147,12 +157,14 @@ __global__ void k_density_adv(dv_params P, DevGrid G, dv_fields F, const dv_coun
     float da = F.density[i] + P.dt * delta;
     da = fmaxf(da, P.density0);
     F.density_adv[i] = da;
-    if (part) {
+    if (part || err_out) {
       float term = P.has_transit ? transit_weight(P, xi.x) * (da - P.density0) : (da - P.density0);
       err = (double)term;
     }
   }
-  if (part) {
+  if (err_out) {
+    if (live) err_out[i] = err;
+  } else if (part) {
     double s = block_sum<double>(err);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
   }
@@ -183,9 +195,10 @@ __global__ void k_density_error(dv_params P, dv_fields F, const dv_counters* __r
 // divergence_solver_iteration_kernel (dimcv_sph.py:421-468)
 template <int D>
 __global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                  const int32_t* __restrict__ done) {
-  if (done && *done) return;
+                                  const int32_t* __restrict__ done, const int32_t* __restrict__ scene) {
+  if (done && (scene ? done[P.n_scenes] : *done)) return;
   FOR_I;
+  if (scene && done && done[scene[i]]) return;
   if (F.material[i] != DV_MATERIAL_FLUID) return;
   V3 xi = ldv<D>(F.x, i);
   float b_i = F.density_adv[i];
@@ -235,9 +248,10 @@ __global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_
 // updated pair by pair (the reference writes v[p_i] inside the task).
 template <int D>
 __global__ void k_pressure_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                const int32_t* __restrict__ done) {
-  if (done && *done) return;
+                                const int32_t* __restrict__ done, const int32_t* __restrict__ scene) {
+  if (done && (scene ? done[P.n_scenes] : *done)) return;
   FOR_I;
+  if (scene && done && done[scene[i]]) return;
   if (F.material[i] != DV_MATERIAL_FLUID) return;
   V3 xi = ldv<D>(F.x, i);
   V3 vi = ldv<D>(F.v, i);
@@ -430,14 +444,14 @@ DV_API int dv_scale_factor(dv_ctx* c, const dv_fields* f, float s) {
 DV_API int dv_density_change(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_density_change, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (double*)nullptr);
+           (double*)nullptr, (const int32_t*)nullptr, (double*)nullptr);
   return DV_OK;
 }
 
 DV_API int dv_density_adv(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_density_adv, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (double*)nullptr);
+           (double*)nullptr, (const int32_t*)nullptr, (double*)nullptr);
   return DV_OK;
 }
 
@@ -455,13 +469,15 @@ DV_API int dv_density_error(dv_ctx* c, const dv_fields* f, float offset, double*
 
 DV_API int dv_divergence_iteration(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_divergence_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
+  LAUNCH_D(k_divergence_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
+           (const int32_t*)nullptr);
   return DV_OK;
 }
 
 DV_API int dv_pressure_iteration(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
+  LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
+           (const int32_t*)nullptr);
   return DV_OK;
 }
 
@@ -480,13 +496,15 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
     int m = std::min(chunk, max_iter - launched);
     for (int k = 0; k < m; ++k) {
       if (which == 0) {
-        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
+        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                 (const int32_t*)nullptr);
         LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 c->red_part);
+                 c->red_part, (const int32_t*)nullptr, (double*)nullptr);
       } else {
-        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
+        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                 (const int32_t*)nullptr);
         LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 c->red_part);
+                 c->red_part, (const int32_t*)nullptr, (double*)nullptr);
       }
       k_solve_finalize<<<1, 1024, 0, c->stream>>>(c->red_part, nb, c->d_cnt, done, eta, max_iter,
                                                   which);
@@ -495,6 +513,44 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
     launched += m;
     if (launched >= max_iter) break;
     DV_CK(c, cudaMemcpyAsync(c->h_flag, done, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DV_CK(c, cudaStreamSynchronize(c->stream));
+    if (*c->h_flag) break;
+    chunk *= 2;
+  }
+  return DV_OK;
+}
+
+// Scene batch: the same Jacobi iteration with per-scene convergence.  While a
+// graph is being captured every iteration up to max_iter is enqueued (the
+// kernels of converged scenes return at once); otherwise the host polls the
+// every-scene-done flag after chunks of 2, 4, 8, ... iterations.
+int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which) {
+  dv_batch_state* b = c->batch;
+  const int nb = nblk(c);
+  const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
+  const int32_t* scene = c->scene_ptr;
+  if (!scene) return dv_fail(c, DV_EINVAL, "dv_batch_solve: no scene ids (grid not built)");
+  int rc = dv_batch_solve_reset(c, which);
+  if (rc) return rc;
+  int launched = 0, chunk = 2;
+  while (launched < max_iter) {
+    const int m = b->capturing ? max_iter : std::min(chunk, max_iter - launched);
+    for (int k = 0; k < m; ++k) {
+      if (which == 0) {
+        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done, scene);
+        LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done,
+                 (double*)nullptr, scene, b->d_err);
+      } else {
+        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done, scene);
+        LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done,
+                 (double*)nullptr, scene, b->d_err);
+      }
+      rc = dv_batch_solve_finalize(c, which);
+      if (rc) return rc;
+    }
+    launched += m;
+    if (launched >= max_iter) break;
+    DV_CK(c, cudaMemcpyAsync(c->h_flag, b->d_done + b->S, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DV_CK(c, cudaStreamSynchronize(c->stream));
     if (*c->h_flag) break;
     chunk *= 2;

@@ -382,16 +382,17 @@ __device__ __forceinline__ int wrap_cell(const dv_params& P, int g, int d) {
   return g < 0 ? g + n : (g >= n ? g - n : g);
 }
 
+// Near-sample correction and finalize of target t (slot i): removes from the
+// main loop's sum the samples within h (cell window, classification
+// r2 <= far_r2_limit), counts the rest, scales by (S - S_i)/count and
+// applies the gate.  M, kden_sum: the scene's sample count and kden_sum;
+// sk: the scene prefix of the cell keys (0 for a single scene).
 template <int D, bool BLOB, bool PER>
-__global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
-                          const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
-                          const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
-                          const float4* __restrict__ near_v, const float* __restrict__ near_S) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nt = C->n_targets;
-  if (t >= nt) return;
-  const int M = C->num_samples;
-  const int i = targets[t];
+__device__ __forceinline__ void far_fix_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                            const dv_solver_fields& S, int t, int i, int M, float kden_sum,
+                                            uint32_t sk, const int32_t* __restrict__ mult,
+                                            const float4* __restrict__ far_acc, const float4* __restrict__ near_v,
+                                            const float* __restrict__ near_S) {
   const V3 xi = ldv<D>(F.x, i);
   const float lim = P.far_r2_limit, d2 = P.blob_delta2;
   const float3 bx = make_float3(P.box[0], P.box[1], P.box[2]);
@@ -406,7 +407,7 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
     for (int b = lo1; b <= hi1; ++b) {
       const uint32_t kab = ka | __ldg(G.mt1 + wrap_cell(P, b, 1));
       for (int cc = lo2; cc <= hi2; ++cc) {
-        const uint32_t key = D == 3 ? (kab | __ldg(G.mt2 + wrap_cell(P, cc, 2))) : kab;
+        const uint32_t key = (D == 3 ? (kab | __ldg(G.mt2 + wrap_cell(P, cc, 2))) : kab) | sk;
         const int s0 = __ldg(G.start + key), e0 = __ldg(G.end + key);
         for (int j = s0; j < e0; ++j) {
           const int m = mult[j];
@@ -430,7 +431,7 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
   }
   const int cnt = M - near_cnt;
   const float coef = BLOB ? P.blob_coef : P.vvpe_coef;
-  const float fac = C->kden_sum_f32 - near_S[t];
+  const float fac = kden_sum - near_S[t];
   V3 fv{0.f, 0.f, 0.f};
   if (cnt > 0) {
     const float sc = coef / (float)cnt;
@@ -450,6 +451,95 @@ __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields 
     v.y = __fadd_rn(v.y, vv.y);
     if (D == 3) v.z = __fadd_rn(v.z, vv.z);
     stv<D>(F.v, i, v);
+  }
+}
+
+template <int D, bool BLOB, bool PER>
+__global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                          const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
+                          const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
+                          const float4* __restrict__ near_v, const float* __restrict__ near_S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C->n_targets) return;
+  far_fix_one<D, BLOB, PER>(P, G, F, S, t, targets[t], C->num_samples, C->kden_sum_f32, 0u, mult, far_acc, near_v,
+                            near_S);
+}
+
+// scene batch: the target's scene gives M, kden_sum and the key prefix
+template <int D, bool BLOB>
+__global__ void k_far_fix_b(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                            const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
+                            const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
+                            const float4* __restrict__ near_v, const float* __restrict__ near_S,
+                            const dv_scene_state* __restrict__ st) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C->n_targets) return;
+  const int i = targets[t];
+  const int sc = F.object_id[i];
+  far_fix_one<D, BLOB, false>(P, G, F, S, t, i, st[sc].num_samples, st[sc].kden_sum_f32,
+                              (uint32_t)sc << G.scene_shift, mult, far_acc, near_v, near_S);
+}
+
+// scene batch main loop: block b is tile b - tile_off_s of the scene s with
+// tile_off_s <= b; its targets [t_start_s + tile·FT2·TT, ...) of the scene
+// run over the scene's samples [m_off_s, m_off_s + M_s) in the order and
+// tiling of k_far_main
+template <int D, int TT, bool BLOB, bool COMP>
+__global__ void __launch_bounds__(FT2) k_far_main_b(dv_params P, const float* __restrict__ x,
+                                                    const int32_t* __restrict__ targets,
+                                                    const float4* __restrict__ spos,
+                                                    const float4* __restrict__ sw,
+                                                    const dv_scene_state* __restrict__ st, int S,
+                                                    const int32_t* __restrict__ ntiles,
+                                                    float4* __restrict__ far_acc) {
+  __shared__ float4 s_p[FTILE2];
+  __shared__ float4 s_w[FTILE2];
+  const int blk = blockIdx.x;
+  if (blk >= *ntiles) return;  // uniform per CTA
+  int lo = 0, hi = S;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (st[mid].tile_off <= blk)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  const int sc = lo - 1;
+  const int t0 = st[sc].t_start, nt = st[sc].n_targets;
+  const int m0 = st[sc].m_off, M = st[sc].num_samples;
+  const int tbase = (blk - st[sc].tile_off) * FT2 * TT;
+  float px[TT], py[TT], pz[TT];
+  Acc<COMP> ax[TT], ay[TT], az[TT];
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    const int t = tbase + k * FT2 + threadIdx.x;
+    V3 xi = ldv<D>(x, targets[t0 + (t < nt ? t : nt - 1)]);
+    px[k] = xi.x;
+    py[k] = xi.y;
+    pz[k] = xi.z;
+  }
+  const float lim = P.far_r2_limit;
+  const float d2 = P.blob_delta2;
+  for (int base = 0; base < M; base += FTILE2) {
+    const int m = min(FTILE2, M - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT2) {
+      s_p[q] = spos[m0 + base + q];
+      s_w[q] = sw[m0 + base + q];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < m; ++q) {
+      const float4 sp = s_p[q];
+      const float4 w = s_w[q];
+#pragma unroll
+      for (int k = 0; k < TT; ++k) far_accum<D, BLOB, COMP, false>(px[k], py[k], pz[k], sp, w, lim, d2, ax[k], ay[k], az[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < TT; ++k) {
+    const int t = tbase + k * FT2 + threadIdx.x;
+    if (t < nt) far_acc[t0 + t] = make_float4(ax[k].val(), ay[k].val(), az[k].val(), 0.0f);
   }
 }
 
@@ -655,6 +745,67 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
     k_prof_pairs<<<1, 1, 0, c->stream>>>(c->d_cnt, c->d_prof);
     DV_LAUNCHED(c);
   }
+  return DV_OK;
+}
+
+int dv_far_tile_width(const dv_ctx* c) { return FT2 * (c->far_tt <= 2 ? 2 : (c->far_tt <= 4 ? 4 : 8)); }
+
+template <int D, bool BLOB, bool COMP>
+static void launch_main_b(dv_ctx* c, const dv_fields* f) {
+  dv_batch_state* b = c->batch;
+  const int nb = (int)b->cap_tiles;
+#define L(TTV)                                                                                             \
+  k_far_main_b<D, TTV, BLOB, COMP><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw,      \
+                                                              b->d_state, b->S, b->d_misc, c->far_acc)
+  if (c->far_tt <= 2)
+    L(2);
+  else if (c->far_tt <= 4)
+    L(4);
+  else
+    L(8);
+#undef L
+}
+
+// Scene batch VVPE: the targets are built (dv_build_targets) and the samples
+// drawn (dv_batch_draw); near field and packing are the single-scene kernels
+int dv_batch_vvpe(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
+  dv_batch_state* b = c->batch;
+  if (!fast_kernel_ok(c->p) && c->p.kernel_mode != DV_KERNEL_BLOB3D)
+    return dv_fail(c, DV_EUNSUPPORTED, "scene batches need h > 1.05e-4 (reference kernel)");
+  int rc = dv_launch_vvpe_near(c, f, s);
+  if (rc) return rc;
+  const int packb = c->num_sms * 4;
+  if (c->p.dim == 2)
+    k_pack_samples<2><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw, c->p.kden_eps);
+  else
+    k_pack_samples<3><<<packb, DV_THREADS, 0, c->stream>>>(*f, *s, c->d_cnt, c->spos, c->sw, c->p.kden_eps);
+  DV_LAUNCHED(c);
+  DV_CK(c, cudaMemsetAsync(c->mult, 0, sizeof(int32_t) * c->cap, c->stream));
+  k_mult<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(s->sample_idx, c->d_cnt, c->mult);
+  DV_LAUNCHED(c);
+  const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D, comp = c->p.compensated != 0;
+#define LB(DD)                                                                             \
+  if (blob)                                                                                \
+    comp ? launch_main_b<DD, true, true>(c, f) : launch_main_b<DD, true, false>(c, f);     \
+  else                                                                                     \
+    comp ? launch_main_b<DD, false, true>(c, f) : launch_main_b<DD, false, false>(c, f);
+  if (c->p.dim == 2) {
+    LB(2);
+  } else {
+    LB(3);
+  }
+#undef LB
+  DV_LAUNCHED(c);
+  const int nb = dv_blocks(c->cap, 128);
+#define LF(DD, B)                                                                                         \
+  k_far_fix_b<DD, B><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,   \
+                                                c->far_acc, c->near_v, c->near_S, b->d_state)
+  if (c->p.dim == 2)
+    blob ? LF(2, true) : LF(2, false);
+  else
+    blob ? LF(3, true) : LF(3, false);
+#undef LF
+  DV_LAUNCHED(c);
   return DV_OK;
 }
 

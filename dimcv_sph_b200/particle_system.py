@@ -53,7 +53,7 @@ class ParticleSystem:
     material_fluid = MATERIAL_FLUID
 
     def __init__(self, config, GGUI=False, device=None, options: Options | None = None,
-                 capacity: int | None = None, verbose: bool = False):
+                 capacity: int | None = None, verbose: bool = False, grid_num=None):
         self.cfg = config
         self.GGUI = GGUI  # accepted for signature compatibility; nothing is drawn
         self.verbose = verbose
@@ -125,6 +125,11 @@ class ParticleSystem:
         # into the other) and the index-stable solver fields
         self.options = options or Options.from_config(config)
         self.params = make_params(config, self.options)
+        if grid_num is not None:  # a larger cell grid (same Morton layout as a scene batch)
+            for d in range(self.dim):
+                if int(grid_num[d]) < self.params.grid_num[d]:
+                    raise ValueError("grid_num may only enlarge the cell grid")
+                self.params.grid_num[d] = int(grid_num[d])
         cap = int(self.particle_max_num)
         self._sets = [particle_fields(cap, self.dim, self.device), particle_fields(cap, self.dim, self.device)]
         self._cur = 0

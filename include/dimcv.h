@@ -135,7 +135,10 @@ typedef struct dv_params {
    * (cells at least h wide) and grid_num[d] >= 3; distances use the minimum image */
   int32_t periodic;
   float box[3];
-  int32_t reserved[4];
+  /* scene batch (new): n_scenes > 1 reserves the top bits of the cell key for
+   * a scene id (dv_batch_*); grid_num is then the largest scene grid */
+  int32_t n_scenes;
+  int32_t reserved[3];
 } dv_params;
 
 /* Fields that travel with a particle: dv_grid_build permutes them
@@ -415,5 +418,69 @@ DV_API int dv_vpm_velocity(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precisi
 DV_API int dv_vpm_velocity_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                                const void* w_s, const void* g_u, void* g_ws, void* g_x, void* workspace,
                                int64_t workspace_bytes);
+
+/* ------------------------------------------------------------------------
+ * Scene batch (new: the reference steps one scene per process).  One context
+ * created with params.n_scenes = S > 1 holds S independent scenes that share
+ * every dv_params constant except the box: particle slots carry their scene
+ * id in object_id, positions are scene-local, the cell key puts the scene id
+ * above the Morton bits (params.grid_num = the largest scene grid), so every
+ * neighbour sweep of the single-scene path runs on the whole batch at once
+ * and never crosses scenes.  The per-scene parts are: activity box, emitter
+ * schedule, DFSPH convergence (each scene iterates until its own average
+ * error passes, as a lone scene would), kden_sum, the sampler
+ * (M_s = max(1, floor(mc_fraction · fluid_s)) stratified draws from the
+ * scene's own CDF with the scene's seed) and the far field (scene targets
+ * against scene samples).  dv_batch_step enqueues one whole step
+ * (karman_vortex.py:216-242 without the export sweep) with no host
+ * synchronisation, so it can be captured in a CUDA graph (dv_batch_graph_*).
+ * ------------------------------------------------------------------------ */
+typedef struct dv_batch_scene {
+  float domain_end[3];    /* the scene's box is [params.domain_start, domain_end] */
+  int32_t cap;            /* upper bound of the scene's particle count */
+  int32_t emit_offset;    /* the scene's emitter particles: [emit_offset, +emit_count) of emit_pos */
+  int32_t emit_count;
+  int32_t emit_interval;  /* emit every emit_interval steps (dimcv_sph.py:66-74); 0: no emitter */
+  float emit_velocity[3];
+  float emit_density;
+  int32_t emit_color[3];
+  float emit_volume;      /* m_V of emitted particles, 0.8 (2r)^dim as f32 (particle_system.py:46) */
+  int32_t pad;
+  uint64_t seed;          /* sampler seed of the scene */
+} dv_batch_scene;
+
+typedef struct dv_scene_state {  /* per scene, device-resident; read with dv_batch_read */
+  int32_t start, end;            /* sorted slot range of the scene's active particles */
+  int32_t n_fluid, n_solid;
+  int32_t t_start, n_targets;    /* range in the target list */
+  int32_t m_off, num_samples;    /* range in sample_idx */
+  int32_t tile_off, iters_div;
+  int32_t iters_p, done;
+  int32_t status, emitted;       /* DV_WARN_* bits of the scene; particles emitted so far */
+  double err_div, err_p, kden_sum;
+  float kden_sum_f32;
+  int32_t pad;
+} dv_scene_state;
+
+/* Per-scene tables; emit_pos is [n_emit][dim] (host); sample_mode is
+ * DV_SAMPLE_INVERSE_CDF or DV_SAMPLE_STRATIFIED.  Sets the device step counter
+ * to 0.  Synchronises. */
+DV_API int dv_batch_setup(dv_ctx* ctx, const dv_batch_scene* scenes, int32_t n_scenes, const float* emit_pos,
+                          int32_t n_emit, float mc_fraction, int32_t sample_mode);
+/* One step of every scene: emit (scenes whose interval divides the step
+ * counter), update_activity, grid build src -> dst, then the substep on dst
+ * (densities, DFSPH factor, divergence solve, non-pressure forces, DIMCV with
+ * stratified sampling, predict, pressure solve, advect); step counter += 1. */
+DV_API int dv_batch_step(dv_ctx* ctx, const dv_fields* src, const dv_fields* dst, const dv_solver_fields* s);
+/* Captures `steps` (even) steps alternating src -> dst, dst -> src into a CUDA
+ * graph owned by the context (replaces the previous one). */
+DV_API int dv_batch_graph_capture(dv_ctx* ctx, const dv_fields* a, const dv_fields* b,
+                                  const dv_solver_fields* s, int32_t steps);
+/* Launches the captured graph once, ordered after the work already on the
+ * context stream and before the work enqueued after it. */
+DV_API int dv_batch_graph_launch(dv_ctx* ctx);
+/* Copies the per-scene state to the host and the device step counter to
+ * *step (may be NULL).  Synchronises. */
+DV_API int dv_batch_read(dv_ctx* ctx, dv_scene_state* out, int32_t n_scenes, int64_t* step);
 
 #endif /* DIMCV_H_ */

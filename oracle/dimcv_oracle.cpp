@@ -304,6 +304,12 @@ DVO_API void dvo_abi_layout(int64_t* out) {
   out[5] = offsetof(dv_params, compensated);
   out[6] = offsetof(dv_counters, err_div);
   out[7] = offsetof(dv_counters, kden_sum_f32);
+  out[8] = sizeof(dv_vpm_plan);
+  out[9] = sizeof(dv_batch_scene);
+  out[10] = offsetof(dv_batch_scene, seed);
+  out[11] = sizeof(dv_scene_state);
+  out[12] = offsetof(dv_scene_state, err_div);
+  out[13] = offsetof(dv_params, n_scenes);
 }
 DVO_API void dvo_set_counts(void* h, int n, int nf, int ns) {
   Ctx* c = (Ctx*)h;

@@ -52,7 +52,7 @@ def test_struct_layout_matches_c():
     from oracle.oracle import load
     lib = load()
     lib.dvo_abi_layout.argtypes = [C.c_void_p]
-    out = np.zeros(8, dtype=np.int64)
+    out = np.zeros(14, dtype=np.int64)
     lib.dvo_abi_layout(out.ctypes.data)
     assert out[0] == C.sizeof(_abi.DvParams)
     assert out[1] == C.sizeof(_abi.DvFields)
@@ -62,3 +62,9 @@ def test_struct_layout_matches_c():
     assert out[5] == _abi.DvParams.compensated.offset
     assert out[6] == _abi.DvCounters.err_div.offset
     assert out[7] == _abi.DvCounters.kden_sum_f32.offset
+    assert out[8] == C.sizeof(_abi.DvVpmPlan)
+    assert out[9] == C.sizeof(_abi.DvBatchScene)
+    assert out[10] == _abi.DvBatchScene.seed.offset
+    assert out[11] == C.sizeof(_abi.DvSceneState)
+    assert out[12] == _abi.DvSceneState.err_div.offset
+    assert out[13] == _abi.DvParams.n_scenes.offset
