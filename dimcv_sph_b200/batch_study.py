@@ -75,6 +75,8 @@ def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lon
                     "iters_p_max": max(s["iters_p"] for s in st2),
                     "iters_p_mean": float(np.mean([s["iters_p"] for s in st2])),
                     "not_converged": sum(1 for s in st2 if s["status"] & 3)}
+    pairs = float(sum(s["n_targets"] * s["num_samples"] for s in st2))
+    out["batch"]["far_pairs_per_step"] = pairs
     sizes = [s["n_fluid"] for s in st2]
     out["scene_fluid_min_median_max"] = [int(np.min(sizes)), int(np.median(sizes)), int(np.max(sizes))]
     del b

@@ -16,6 +16,24 @@
 
 namespace {
 
+// exclusive scan of v over the threads of one block (blockDim.x <= 1024);
+// returns the thread's offset, *total gets the sum
+__device__ __forceinline__ int block_excl_scan(int v, int* total) {
+  __shared__ int part[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  __syncthreads();
+  part[tid] = v;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {  // inclusive Hillis-Steele scan
+    const int u = tid >= o ? part[tid - o] : 0;
+    __syncthreads();
+    part[tid] += u;
+    __syncthreads();
+  }
+  *total = part[nt - 1];
+  return part[tid] - v;
+}
+
 // ---------------------------------------------------------------- emission
 // emit_particle (dimcv_sph.py:616-637) for every scene whose interval
 // divides the step counter: its emitter lattice is appended after the
@@ -26,14 +44,22 @@ __global__ void k_batch_emit(dv_fields F, const dv_batch_scene* __restrict__ sc,
                              int cap, dv_scene_state* st) {
   extern __shared__ int off[];  // [S + 1]
   const int64_t t = *step;
-  if (threadIdx.x == 0) {
-    int o = 0;
-    for (int s = 0; s < S; ++s) {
+  {
+    const int per = (S + blockDim.x - 1) / blockDim.x;
+    const int s0 = min(S, (int)threadIdx.x * per), s1 = min(S, s0 + per);
+    int mine = 0;
+    for (int s = s0; s < s1; ++s) {
+      const int iv = sc[s].emit_interval;
+      if (iv > 0 && sc[s].emit_count > 0 && t % iv == 0) mine += sc[s].emit_count;
+    }
+    int total;
+    int o = block_excl_scan(mine, &total);
+    for (int s = s0; s < s1; ++s) {
       off[s] = o;
       const int iv = sc[s].emit_interval;
       if (iv > 0 && sc[s].emit_count > 0 && t % iv == 0) o += sc[s].emit_count;
     }
-    off[S] = o;
+    if (threadIdx.x == 0) off[S] = total;
   }
   __syncthreads();
   const int n0 = C->n, total = off[S];
@@ -148,14 +174,14 @@ __global__ void k_batch_kden(dv_params P, dv_fields F, const float* __restrict__
 }
 
 // target, sample and far-field tile offsets; M_s = max(1, floor(frac · fluid_s))
-// where the scene has targets with a positive kden_sum, else 0 (dv_sample)
+// where the scene has targets with a positive kden_sum, else 0 (dv_sample).
+// One block; each thread owns a contiguous run of scenes.
 __global__ void k_batch_offsets(dv_scene_state* st, int S, float frac, int tile_w, dv_counters* C,
                                 int32_t* misc) {
+  const int per = (S + blockDim.x - 1) / blockDim.x;
+  const int s0 = min(S, (int)threadIdx.x * per), s1 = min(S, s0 + per);
   int t = 0, m = 0, tiles = 0;
-  for (int s = 0; s < S; ++s) {
-    st[s].t_start = t;
-    st[s].m_off = m;
-    st[s].tile_off = tiles;
+  for (int s = s0; s < s1; ++s) {
     const int nt = st[s].n_targets;
     int M = 0;
     if (nt > 0 && st[s].kden_sum > 0.0) {
@@ -167,12 +193,26 @@ __global__ void k_batch_offsets(dv_scene_state* st, int S, float frac, int tile_
     m += M;
     tiles += (nt + tile_w - 1) / tile_w;
   }
-  C->num_samples = m;
-  misc[0] = tiles;
+  int tt, mt, ct;
+  int ot = block_excl_scan(t, &tt);
+  int om = block_excl_scan(m, &mt);
+  int oc = block_excl_scan(tiles, &ct);
+  for (int s = s0; s < s1; ++s) {
+    st[s].t_start = ot;
+    st[s].m_off = om;
+    st[s].tile_off = oc;
+    ot += st[s].n_targets;
+    om += st[s].num_samples;
+    oc += (st[s].n_targets + tile_w - 1) / tile_w;
+  }
+  if (threadIdx.x == 0) {
+    C->num_samples = mt;
+    misc[0] = ct;
+  }
 }
 
 // ----------------------------------------------------------- DFSPH solves
-__global__ void k_batch_solve_reset(dv_scene_state* st, int32_t* done, int S, int which) {
+__global__ void k_batch_solve_reset(dv_scene_state* st, int32_t* done, int S, int which, int32_t* ctr) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < S) {
     done[s] = 0;
@@ -181,18 +221,21 @@ __global__ void k_batch_solve_reset(dv_scene_state* st, int32_t* done, int S, in
     else
       st[s].iters_p = 0;
   }
-  if (s == 0) done[S] = 0;
+  if (s == 0) {
+    done[S] = 0;
+    *ctr = 0;
+  }
 }
 
-// k_solve_finalize per scene: FP64 sum of the scene's residual terms, average
-// over its fluid count, convergence test against eta or the iteration cap
-__global__ void k_batch_solve_finalize(const double* __restrict__ err, dv_scene_state* st, int32_t* done,
-                                       double eta, int max_iter, int which) {
+// k_solve_finalize per scene: FP64 sum of the scene's residual block sums
+// (part[wl[s] .. wl[s+1]) of the iteration's work list), average over its
+// fluid count, convergence test against eta or the iteration cap
+__global__ void k_batch_solve_finalize(const double* __restrict__ part, const int32_t* __restrict__ wl,
+                                       dv_scene_state* st, int32_t* done, double eta, int max_iter, int which) {
   const int s = blockIdx.x;
   if (done[s]) return;
-  const int a = st[s].start, b = st[s].end;
   double acc = 0.0;
-  for (int i = a + threadIdx.x; i < b; i += blockDim.x) acc += err[i];
+  for (int k = wl[s] + threadIdx.x; k < wl[s + 1]; k += blockDim.x) acc += part[k];
   acc = block_sum<double>(acc);
   if (threadIdx.x == 0) {
     const int nf = st[s].n_fluid;
@@ -212,11 +255,46 @@ __global__ void k_batch_solve_finalize(const double* __restrict__ err, dv_scene_
   }
 }
 
-__global__ void k_batch_all_done(int32_t* done, int S) {
-  int all = 1;
-  for (int s = threadIdx.x; s < S; s += blockDim.x) all &= done[s] != 0;
-  all = block_sum<int>(all);
-  if (threadIdx.x == 0) done[S] = all == (int)blockDim.x ? 1 : 0;  // threads without a scene count 1
+// work list of the scenes still iterating: wl[s] = first block of scene s
+// (blocks of DV_THREADS slots), wl[S] = total; done[S] = nothing left.
+// One block; each thread owns a contiguous run of scenes.
+__global__ void k_batch_worklist(const dv_scene_state* __restrict__ st, int32_t* done, int S,
+                                 int32_t* __restrict__ wl) {
+  __shared__ int part[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int per = (S + nt - 1) / nt;
+  const int s0 = min(S, tid * per), s1 = min(S, s0 + per);
+  int sum = 0;
+  for (int s = s0; s < s1; ++s) {
+    const int n = st[s].end - st[s].start;
+    if (!done[s] && n > 0) sum += (n + DV_THREADS - 1) / DV_THREADS;
+  }
+  part[tid] = sum;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {  // inclusive Hillis-Steele scan
+    const int v = tid >= o ? part[tid - o] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int off = part[tid] - sum;
+  for (int s = s0; s < s1; ++s) {
+    wl[s] = off;
+    const int n = st[s].end - st[s].start;
+    if (!done[s] && n > 0) off += (n + DV_THREADS - 1) / DV_THREADS;
+  }
+  if (tid == nt - 1) {
+    wl[S] = part[nt - 1];
+    done[S] = part[nt - 1] == 0 ? 1 : 0;
+  }
+}
+
+// condition of the captured Jacobi loop: continue while a scene iterates,
+// at most max_iter times (own counter, independent of the data)
+__global__ void k_batch_cond(cudaGraphConditionalHandle h, const int32_t* __restrict__ wl, int S, int32_t* ctr,
+                             int max_iter) {
+  const int it = ++*ctr;
+  cudaGraphSetConditional(h, (wl[S] > 0 && it < max_iter) ? 1u : 0u);
 }
 
 __global__ void k_batch_step_inc(int64_t* step) { *step += 1; }
@@ -231,7 +309,17 @@ int check_batch(dv_ctx* c) {
 
 int dv_batch_solve_reset(dv_ctx* c, int which) {
   dv_batch_state* b = c->batch;
-  k_batch_solve_reset<<<dv_blocks(b->S), DV_THREADS, 0, c->stream>>>(b->d_state, b->d_done, b->S, which);
+  k_batch_solve_reset<<<dv_blocks(b->S), DV_THREADS, 0, c->stream>>>(b->d_state, b->d_done, b->S, which,
+                                                                      b->d_ctr);
+  DV_LAUNCHED(c);
+  k_batch_worklist<<<1, 1024, 0, c->stream>>>(b->d_state, b->d_done, b->S, b->d_wl);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+int dv_batch_loop_condition(dv_ctx* c, cudaGraphConditionalHandle h, int max_iter) {
+  dv_batch_state* b = c->batch;
+  k_batch_cond<<<1, 1, 0, c->stream>>>(h, b->d_wl, b->S, b->d_ctr, max_iter);
   DV_LAUNCHED(c);
   return DV_OK;
 }
@@ -240,10 +328,10 @@ int dv_batch_solve_finalize(dv_ctx* c, int which) {
   dv_batch_state* b = c->batch;
   const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
   const double eta = which == 0 ? c->p.eta_div : c->p.eta_p;
-  k_batch_solve_finalize<<<b->S, DV_THREADS, 0, c->stream>>>(b->d_err, b->d_state, b->d_done, eta, max_iter,
-                                                              which);
+  k_batch_solve_finalize<<<b->S, DV_THREADS, 0, c->stream>>>(b->d_err, b->d_wl, b->d_state, b->d_done, eta,
+                                                              max_iter, which);
   DV_LAUNCHED(c);
-  k_batch_all_done<<<1, 1024, 0, c->stream>>>(b->d_done, b->S);
+  k_batch_worklist<<<1, 1024, 0, c->stream>>>(b->d_state, b->d_done, b->S, b->d_wl);
   DV_LAUNCHED(c);
   return DV_OK;
 }
@@ -284,6 +372,8 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
   al((void**)&b->d_scenes, sizeof(dv_batch_scene) * n_scenes);
   al((void**)&b->d_state, sizeof(dv_scene_state) * n_scenes);
   al((void**)&b->d_done, sizeof(int32_t) * (n_scenes + 1));
+  al((void**)&b->d_wl, sizeof(int32_t) * (n_scenes + 1));
+  al((void**)&b->d_ctr, sizeof(int32_t));
   al((void**)&b->d_misc, sizeof(int32_t) * 4);
   al((void**)&b->d_err, sizeof(double) * c->cap);
   al((void**)&b->d_step, sizeof(int64_t));
@@ -302,7 +392,10 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
     e = cudaMemcpy(b->d_emit, emit_pos, sizeof(float) * c->p.dim * n_emit, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(c->d_scene_end, ends.data(), sizeof(float) * 3 * n_scenes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->d_wl, 0, sizeof(int32_t) * (n_scenes + 1));
+  if (e == cudaSuccess) e = cudaMemset(b->d_ctr, 0, sizeof(int32_t));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->gstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->bstream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev0, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev1, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -319,9 +412,12 @@ void dv_batch_free(dv_ctx* c) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->gstream) cudaStreamDestroy(b->gstream);
+  if (b->bstream) cudaStreamDestroy(b->bstream);
   cudaFree(b->d_scenes);
   cudaFree(b->d_state);
   cudaFree(b->d_done);
+  cudaFree(b->d_wl);
+  cudaFree(b->d_ctr);
   cudaFree(b->d_misc);
   cudaFree(b->d_err);
   cudaFree(b->d_step);
@@ -360,9 +456,9 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
                                                                   S, b->d_state);
   DV_LAUNCHED(c);
   if (c->p.dim == 2)
-    k_batch_counts<2><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, b->d_state);
+    k_batch_counts<2><<<S, 1024, 0, c->stream>>>(c->p, *dst, b->d_state);
   else
-    k_batch_counts<3><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, b->d_state);
+    k_batch_counts<3><<<S, 1024, 0, c->stream>>>(c->p, *dst, b->d_state);
   DV_LAUNCHED(c);
   // substep (karman_vortex.py:232-242)
   DV_TRY(dv_densities(c, dst));
@@ -378,12 +474,12 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
   DV_TRY(dv_kvn_sample(c, dst, s, 0, 0, 0));
   DV_TRY(dv_akde(c, dst, s));
   if (c->p.dim == 2)
-    k_batch_kden<2><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
+    k_batch_kden<2><<<S, 1024, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
   else
-    k_batch_kden<3><<<S, DV_THREADS, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
+    k_batch_kden<3><<<S, 1024, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
   DV_LAUNCHED(c);
-  k_batch_offsets<<<1, 1, 0, c->stream>>>(b->d_state, S, b->mc_fraction, dv_far_tile_width(c), c->d_cnt,
-                                          b->d_misc);
+  k_batch_offsets<<<1, 1024, 0, c->stream>>>(b->d_state, S, b->mc_fraction, dv_far_tile_width(c), c->d_cnt,
+                                             b->d_misc);
   DV_LAUNCHED(c);
   DV_TRY(dv_build_targets(c, dst));
   DV_TRY(dv_batch_draw(c, s));

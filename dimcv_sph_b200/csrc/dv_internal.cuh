@@ -144,8 +144,10 @@ struct dv_batch_state {
   dv_batch_scene* d_scenes = nullptr; // [S]
   dv_scene_state* d_state = nullptr;  // [S]
   int32_t* d_done = nullptr;          // [S + 1]: per-scene solve done; [S]: every scene done
+  int32_t* d_wl = nullptr;            // [S + 1]: work list of the scenes still iterating (block offsets)
+  int32_t* d_ctr = nullptr;           // iterations of the captured Jacobi loop
   int32_t* d_misc = nullptr;          // [0]: far-field tiles this step
-  double* d_err = nullptr;            // [cap] per-slot residual terms of the solves
+  double* d_err = nullptr;            // [cap] residual block sums of the solves (one per work-list block)
   int64_t* d_step = nullptr;          // step counter (emission schedule, sampler stream)
   float* d_emit = nullptr;            // [n_emit][dim]
   int32_t n_emit = 0;
@@ -155,12 +157,14 @@ struct dv_batch_state {
   int stratified = 0;                 // DV_SAMPLE_STRATIFIED draws, else i.i.d.
   cudaGraphExec_t graph = nullptr;
   cudaStream_t gstream = nullptr;
+  cudaStream_t bstream = nullptr;     // captures the Jacobi loop bodies
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 // dv_batch.cu
 void dv_batch_free(dv_ctx* c);
 int dv_batch_solve_reset(dv_ctx* c, int which);
 int dv_batch_solve_finalize(dv_ctx* c, int which);
+int dv_batch_loop_condition(dv_ctx* c, cudaGraphConditionalHandle h, int max_iter);
 // dv_sph.cu: one DFSPH Jacobi solve with per-scene convergence
 int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which);
 // dv_dimcv.cu: per-scene inverse-CDF draws (targets built)

@@ -83,88 +83,83 @@ __global__ void k_scale_factor(dv_fields F, float s, const dv_counters* __restri
 }
 
 // ------------------------------------------------------- density change
-// compute_density_change (dimcv_sph.py:337-374); optionally the block
-// partial of compute_density_error(0) (dimcv_sph.py:407-419) in FP64.
-//
-// Scene batch (scene != NULL): done[] is per scene (the slot's scene id),
-// converged scenes are skipped per thread, and the error term of every slot
-// goes to err_out[i] (0 where none) for the per-scene sums.
+// compute_density_change (dimcv_sph.py:337-374) of slot i; returns the
+// compute_density_error(0) term (dimcv_sph.py:407-419), 0 for non-fluid.
+template <int D>
+__device__ __forceinline__ double density_change_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                     int i) {
+  if (F.material[i] != DV_MATERIAL_FLUID) return 0.0;
+  V3 xi = ldv<D>(F.x, i);
+  V3 vi = ldv<D>(F.v, i);
+  float adv = 0.0f;
+  int nn = 0;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      adv += F.m_V[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+    }
+    nn += 1;
+  });
+  float da = fmaxf(adv, 0.0f);
+  if (nn < P.neighbor_min) da = 0.0f;
+  F.density_adv[i] = da;
+  float term = P.has_transit ? transit_weight(P, xi.x) * (da - 0.0f) : (da - 0.0f);
+  return (double)term;
+}
+
+// optionally the FP64 block partial of the error terms
 template <int D>
 __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                 const int32_t* __restrict__ done, double* __restrict__ part,
-                                 const int32_t* __restrict__ scene, double* __restrict__ err_out) {
-  if (done && (scene ? done[P.n_scenes] : *done)) return;  // [n_scenes]: every scene converged
+                                 const int32_t* __restrict__ done, double* __restrict__ part) {
+  if (done && *done) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
-  const bool live = i < C->n && !(scene && done && done[scene[i]]);
-  if (live && F.material[i] == DV_MATERIAL_FLUID) {
-    V3 xi = ldv<D>(F.x, i);
-    V3 vi = ldv<D>(F.v, i);
-    float adv = 0.0f;
-    int nn = 0;
-    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-      int mj = F.material[j];
-      if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
-        V3 vj = ldv<D>(F.v, j);
-        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
-        adv += F.m_V[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
-      }
-      nn += 1;
-    });
-    float da = fmaxf(adv, 0.0f);
-    if (nn < P.neighbor_min) da = 0.0f;
-    F.density_adv[i] = da;
-    if (part || err_out) {
-      float term = P.has_transit ? transit_weight(P, xi.x) * (da - 0.0f) : (da - 0.0f);
-      err = (double)term;
-    }
-  }
-  if (err_out) {
-    if (live) err_out[i] = err;
-  } else if (part) {
+  if (i < C->n) err = density_change_one<D>(P, G, F, i);
+  if (part) {
     double s = block_sum<double>(err);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
   }
 }
 
 // ------------------------------------------------------------ density adv
-// compute_density_adv (dimcv_sph.py:470-493); optionally the block partial of
-// compute_density_error(density0).
+// compute_density_adv (dimcv_sph.py:470-493) of slot i; returns the
+// compute_density_error(density0) term, 0 for non-fluid.
+template <int D>
+__device__ __forceinline__ double density_adv_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                  int i) {
+  if (F.material[i] != DV_MATERIAL_FLUID) return 0.0;
+  V3 xi = ldv<D>(F.x, i);
+  V3 vi = ldv<D>(F.v, i);
+  float delta = 0.0f;
+  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
+    int mj = F.material[j];
+    if (mj == DV_MATERIAL_FLUID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      delta += F.m[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+    } else if (mj == DV_MATERIAL_SOLID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      delta += F.m_V[j] * P.density0 * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+    }
+  });
+  float da = F.density[i] + P.dt * delta;
+  da = fmaxf(da, P.density0);
+  F.density_adv[i] = da;
+  float term = P.has_transit ? transit_weight(P, xi.x) * (da - P.density0) : (da - P.density0);
+  return (double)term;
+}
+
 template <int D>
 __global__ void k_density_adv(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                              const int32_t* __restrict__ done, double* __restrict__ part,
-                              const int32_t* __restrict__ scene, double* __restrict__ err_out) {
-  if (done && (scene ? done[P.n_scenes] : *done)) return;  // [n_scenes]: every scene converged
+                              const int32_t* __restrict__ done, double* __restrict__ part) {
+  if (done && *done) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
-  const bool live = i < C->n && !(scene && done && done[scene[i]]);
-  if (live && F.material[i] == DV_MATERIAL_FLUID) {
-    V3 xi = ldv<D>(F.x, i);
-    V3 vi = ldv<D>(F.v, i);
-    float delta = 0.0f;
-    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-      int mj = F.material[j];
-      if (mj == DV_MATERIAL_FLUID) {
-        V3 vj = ldv<D>(F.v, j);
-        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
-        delta += F.m[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
-      } else if (mj == DV_MATERIAL_SOLID) {
-        V3 vj = ldv<D>(F.v, j);
-        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
-        delta += F.m_V[j] * P.density0 * dot<D>(dv, cubic_gradW<D>(P, r, r2));
-      }
-    });
-    float da = F.density[i] + P.dt * delta;
-    da = fmaxf(da, P.density0);
-    F.density_adv[i] = da;
-    if (part || err_out) {
-      float term = P.has_transit ? transit_weight(P, xi.x) * (da - P.density0) : (da - P.density0);
-      err = (double)term;
-    }
-  }
-  if (err_out) {
-    if (live) err_out[i] = err;
-  } else if (part) {
+  if (i < C->n) err = density_adv_one<D>(P, G, F, i);
+  if (part) {
     double s = block_sum<double>(err);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
   }
@@ -194,11 +189,8 @@ __global__ void k_density_error(dv_params P, dv_fields F, const dv_counters* __r
 // ---------------------------------------------------- Jacobi iterations
 // divergence_solver_iteration_kernel (dimcv_sph.py:421-468)
 template <int D>
-__global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                  const int32_t* __restrict__ done, const int32_t* __restrict__ scene) {
-  if (done && (scene ? done[P.n_scenes] : *done)) return;
-  FOR_I;
-  if (scene && done && done[scene[i]]) return;
+__device__ __forceinline__ void divergence_iter_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                    int i) {
   if (F.material[i] != DV_MATERIAL_FLUID) return;
   V3 xi = ldv<D>(F.x, i);
   float b_i = F.density_adv[i];
@@ -247,11 +239,8 @@ __global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_
 // pressure_solve_iteration_kernel (dimcv_sph.py:495-549): the velocity is
 // updated pair by pair (the reference writes v[p_i] inside the task).
 template <int D>
-__global__ void k_pressure_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
-                                const int32_t* __restrict__ done, const int32_t* __restrict__ scene) {
-  if (done && (scene ? done[P.n_scenes] : *done)) return;
-  FOR_I;
-  if (scene && done && done[scene[i]]) return;
+__device__ __forceinline__ void pressure_iter_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                  int i) {
   if (F.material[i] != DV_MATERIAL_FLUID) return;
   V3 xi = ldv<D>(F.x, i);
   V3 vi = ldv<D>(F.v, i);
@@ -292,6 +281,68 @@ __global__ void k_pressure_iter(dv_params P, DevGrid G, dv_fields F, const dv_co
     }
   });
   stv<D>(F.v, i, vi);
+}
+
+template <int D>
+__global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                  const int32_t* __restrict__ done) {
+  if (done && *done) return;
+  FOR_I;
+  divergence_iter_one<D>(P, G, F, i);
+}
+
+template <int D>
+__global__ void k_pressure_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                const int32_t* __restrict__ done) {
+  if (done && *done) return;
+  FOR_I;
+  pressure_iter_one<D>(P, G, F, i);
+}
+
+// Scene batch forms: a grid of a few blocks per SM walks the work list of
+// the scenes still iterating (wl[s] = first block of scene s, wl[S] = total,
+// blocks of DV_THREADS slots from the scene's start).
+__device__ __forceinline__ int wl_scene(const int32_t* __restrict__ wl, int S, int b) {
+  int lo = 0, hi = S;  // last s with wl[s] <= b
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (wl[mid] <= b)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo - 1;
+}
+
+template <int D, int WHICH>
+__global__ void k_batch_iter(dv_params P, DevGrid G, dv_fields F, const dv_scene_state* __restrict__ st,
+                             const int32_t* __restrict__ wl, int S) {
+  const int tot = wl[S];
+  for (int b = blockIdx.x; b < tot; b += gridDim.x) {
+    const int s = wl_scene(wl, S, b);
+    const int i = st[s].start + (b - wl[s]) * DV_THREADS + threadIdx.x;
+    if (i >= st[s].end) continue;
+    if (WHICH == 0)
+      divergence_iter_one<D>(P, G, F, i);
+    else
+      pressure_iter_one<D>(P, G, F, i);
+  }
+}
+
+// residual sweep: FP64 block sum of the error terms of work-list block b
+// (a block never spans two scenes) into part[b]
+template <int D, int WHICH>
+__global__ void k_batch_residual(dv_params P, DevGrid G, dv_fields F, const dv_scene_state* __restrict__ st,
+                                 const int32_t* __restrict__ wl, int S, double* __restrict__ part) {
+  const int tot = wl[S];
+  for (int b = blockIdx.x; b < tot; b += gridDim.x) {  // block-uniform bounds
+    const int s = wl_scene(wl, S, b);
+    const int i = st[s].start + (b - wl[s]) * DV_THREADS + threadIdx.x;
+    double e = 0.0;
+    if (i < st[s].end) e = WHICH == 0 ? density_change_one<D>(P, G, F, i) : density_adv_one<D>(P, G, F, i);
+    e = block_sum<double>(e);
+    if (threadIdx.x == 0) part[b] = e;
+  }
 }
 
 // convergence test of one Jacobi iteration: average error over the fluid
@@ -444,14 +495,14 @@ DV_API int dv_scale_factor(dv_ctx* c, const dv_fields* f, float s) {
 DV_API int dv_density_change(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_density_change, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (double*)nullptr, (const int32_t*)nullptr, (double*)nullptr);
+           (double*)nullptr);
   return DV_OK;
 }
 
 DV_API int dv_density_adv(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_density_adv, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (double*)nullptr, (const int32_t*)nullptr, (double*)nullptr);
+           (double*)nullptr);
   return DV_OK;
 }
 
@@ -469,15 +520,13 @@ DV_API int dv_density_error(dv_ctx* c, const dv_fields* f, float offset, double*
 
 DV_API int dv_divergence_iteration(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_divergence_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (const int32_t*)nullptr);
+  LAUNCH_D(k_divergence_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
   return DV_OK;
 }
 
 DV_API int dv_pressure_iteration(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr,
-           (const int32_t*)nullptr);
+  LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
   return DV_OK;
 }
 
@@ -496,15 +545,13 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
     int m = std::min(chunk, max_iter - launched);
     for (int k = 0; k < m; ++k) {
       if (which == 0) {
-        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 (const int32_t*)nullptr);
+        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
         LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 c->red_part, (const int32_t*)nullptr, (double*)nullptr);
+                 c->red_part);
       } else {
-        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 (const int32_t*)nullptr);
+        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
         LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 c->red_part, (const int32_t*)nullptr, (double*)nullptr);
+                 c->red_part);
       }
       k_solve_finalize<<<1, 1024, 0, c->stream>>>(c->red_part, nb, c->d_cnt, done, eta, max_iter,
                                                   which);
@@ -520,32 +567,74 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
   return DV_OK;
 }
 
-// Scene batch: the same Jacobi iteration with per-scene convergence.  While a
-// graph is being captured every iteration up to max_iter is enqueued (the
-// kernels of converged scenes return at once); otherwise the host polls the
-// every-scene-done flag after chunks of 2, 4, 8, ... iterations.
+// Scene batch: the same Jacobi iteration with per-scene convergence.  One
+// iteration is (update sweep, residual sweep, per-scene finalize, work list
+// of the scenes still iterating).  Eagerly the host polls after chunks of
+// 2, 4, 8, ... iterations; under graph capture the iteration is the body of
+// a conditional WHILE node whose condition kernel counts its own iterations
+// and stops at max_iter whatever the data, or earlier when every scene has
+// converged.
+static int batch_iteration(dv_ctx* c, const dv_fields* f, int which) {
+  dv_batch_state* b = c->batch;
+  const int grid = c->num_sms * 8;
+  const DevGrid G = dv_grid(c);
+#define LB(K, ...)                                                                           \
+  do {                                                                                       \
+    if (c->p.dim == 2)                                                                       \
+      which == 0 ? K<2, 0><<<grid, DV_THREADS, 0, c->stream>>>(__VA_ARGS__)                 \
+                 : K<2, 1><<<grid, DV_THREADS, 0, c->stream>>>(__VA_ARGS__);                \
+    else                                                                                     \
+      which == 0 ? K<3, 0><<<grid, DV_THREADS, 0, c->stream>>>(__VA_ARGS__)                 \
+                 : K<3, 1><<<grid, DV_THREADS, 0, c->stream>>>(__VA_ARGS__);                \
+    DV_LAUNCHED(c);                                                                          \
+  } while (0)
+  LB(k_batch_iter, c->p, G, *f, b->d_state, b->d_wl, b->S);
+  LB(k_batch_residual, c->p, G, *f, b->d_state, b->d_wl, b->S, b->d_err);
+#undef LB
+  return dv_batch_solve_finalize(c, which);
+}
+
 int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which) {
   dv_batch_state* b = c->batch;
-  const int nb = nblk(c);
   const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
-  const int32_t* scene = c->scene_ptr;
-  if (!scene) return dv_fail(c, DV_EINVAL, "dv_batch_solve: no scene ids (grid not built)");
   int rc = dv_batch_solve_reset(c, which);
   if (rc) return rc;
+  if (b->capturing) {
+    cudaStream_t st = c->stream;
+    cudaStreamCaptureStatus cs;
+    unsigned long long id = 0;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    DV_CK(c, cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return dv_fail(c, DV_EINVAL, "dv_batch_solve: stream not capturing");
+    cudaGraphConditionalHandle h;
+    DV_CK(c, cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    DV_CK(c, cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    DV_CK(c, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    DV_CK(c, cudaStreamBeginCaptureToGraph(b->bstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    c->stream = b->bstream;
+    rc = batch_iteration(c, f, which);
+    if (rc == DV_OK) rc = dv_batch_loop_condition(c, h, max_iter);
+    c->stream = st;
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->bstream, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return dv_cuda_check(c, e, "capture of the Jacobi loop body");
+    return DV_OK;
+  }
   int launched = 0, chunk = 2;
   while (launched < max_iter) {
-    const int m = b->capturing ? max_iter : std::min(chunk, max_iter - launched);
+    const int m = std::min(chunk, max_iter - launched);
     for (int k = 0; k < m; ++k) {
-      if (which == 0) {
-        LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done, scene);
-        LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done,
-                 (double*)nullptr, scene, b->d_err);
-      } else {
-        LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done, scene);
-        LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)b->d_done,
-                 (double*)nullptr, scene, b->d_err);
-      }
-      rc = dv_batch_solve_finalize(c, which);
+      rc = batch_iteration(c, f, which);
       if (rc) return rc;
     }
     launched += m;

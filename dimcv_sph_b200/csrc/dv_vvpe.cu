@@ -279,8 +279,10 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy);
     ax.s = __fmaf_rn(b, w.z, ax.s);
     ay.s = __fmaf_rn(-a, w.z, ay.s);
-    az.s = __fmaf_rn(a, w.y, az.s);
-    az.s = __fmaf_rn(-b, w.x, az.s);
+    if (D == 3) {  // in 2-D ω̃ = (0, 0, ω_z) by construction: the z row is exactly 0
+      az.s = __fmaf_rn(a, w.y, az.s);
+      az.s = __fmaf_rn(-b, w.x, az.s);
+    }
   } else {
     const float inv = rsqrtf(__fadd_rn(r2, d2));
     const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
