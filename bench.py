@@ -279,7 +279,8 @@ def run_ours(args, rank, world, local):
                              l2="state (~1.3 GB) larger than L2; no flush"),
               "clocks": clk, "gpu_launches": int(launches), "roofline": roofline,
               "iterations": {"divergence": cnt1["iters_div"], "pressure": cnt1["iters_p"]},
-              "far_tile_targets_per_thread": solver.far_tile}
+              "far_tile_targets_per_thread": solver.far_tile,
+              "far_sample_chunks": int(ps.lib.dv_get_far_chunks(ps.ctx))}
 
     # per-stage device times and HBM fractions (outside the timed region)
     st = stage_times(solver, ps, 3)

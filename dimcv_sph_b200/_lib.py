@@ -66,6 +66,8 @@ PROTOTYPES = {
     "dv_fp32_peak": (C.c_int, [_P, C.POINTER(f64)]),
     "dv_density_error_noalloc": (C.c_int, [_PP, _FP, i32, f32, C.POINTER(f64), _P]),
     "dv_profile": (C.c_int, [_P, i32]),
+    "dv_set_far_chunks": (C.c_int, [_P, i32]),
+    "dv_get_far_chunks": (i32, [_P]),
     "dv_vpm_workspace_bytes": (i64, [_P, i32, i32, i32]),
     "dv_batch_setup": (C.c_int, [_P, C.POINTER(DvBatchScene), i32, _P, i32, f32, i32]),
     "dv_batch_step": (C.c_int, [_P, _FP, _FP, _SP]),

@@ -115,12 +115,35 @@ def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lon
     return out
 
 
+def profile_window(n_scenes: int = 256, seed: int = 0, warmup: int = 6, steps: int = 2, tile: int = 2):
+    """Eager batch steps bracketed by cudaProfilerStart/Stop, for a profiler
+    started with --profile-from-start off."""
+    cfgs, _ = channel_batch_configs(n_scenes=n_scenes, seed=seed)
+    b = SceneBatch(cfgs)
+    b._check(b.lib.dv_set_far_tile(b.ctx, int(tile)), "dv_set_far_tile")
+    for _ in range(warmup):
+        b.step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for _ in range(steps):
+        b.step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return b.states()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--out", type=str, default=None)
+    ap.add_argument("--profile-window", action="store_true",
+                    help="only run 2 eager steps inside cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     a = ap.parse_args()
+    if a.profile_window:
+        st = profile_window(n_scenes=a.scenes)
+        print(json.dumps({"profiled_steps": 2, "scenes": len(st)}))
+        return
     res = run(n_scenes=a.scenes, reps=a.reps)
     s = json.dumps(res)
     print(s)

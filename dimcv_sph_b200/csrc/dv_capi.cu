@@ -194,7 +194,7 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   A(c->sw, cap);
   A(c->near_v, cap);
   A(c->near_S, cap);
-  A(c->far_acc, cap);
+  A(c->far_acc, cap * DV_MAX_FAR_CHUNKS);
   A(c->mult, cap);
   // neighbour lists: 48 (3-D) / 24 (2-D) entries per particle on average,
   // beyond which the sweeps keep scanning cells

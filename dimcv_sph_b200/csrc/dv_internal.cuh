@@ -16,6 +16,7 @@
 #include "../../include/dimcv.h"
 
 #define DV_THREADS 256
+#define DV_MAX_FAR_CHUNKS 8
 
 // ------------------------------------------------------------------ context
 struct dv_ctx {
@@ -66,6 +67,7 @@ struct dv_ctx {
   float4* far_acc = nullptr;   // cap: far-field sums of the main loop, per target
   int32_t* mult = nullptr;     // cap: sample multiplicity per slot
   int far_tt = 4;              // targets per thread of the far-field main loop (autotuned)
+  int far_chunks = 1;          // sample chunks of the far-field grid (autotuned, <= DV_MAX_FAR_CHUNKS)
 
   // per-step neighbour lists (CSR, visit order) built by dv_grid_build
   uint32_t* nbr_off = nullptr;  // cap + 1

@@ -299,17 +299,29 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
 #define FT2 256
 #define FTILE2 512
 
+// sample chunk blockIdx.y of nchunk: [m0, m0 + M) of the M_total samples;
+// the chunk's partial sums go to far_acc[chunk * stride + t]
+__device__ __forceinline__ void sample_chunk(int M_total, int nchunk, int& m0, int& M) {
+  const int clen = (M_total + nchunk - 1) / nchunk;
+  m0 = (int)blockIdx.y * clen;
+  M = max(0, min(clen, M_total - m0));
+}
+
 template <int D, int TT, bool BLOB, bool COMP, bool PER>
 __global__ void __launch_bounds__(FT2) k_far_main(dv_params P, const float* __restrict__ x,
                                                   const dv_counters* __restrict__ C,
                                                   const int32_t* __restrict__ targets,
                                                   const float4* __restrict__ spos,
                                                   const float4* __restrict__ sw,
-                                                  float4* __restrict__ far_acc) {
+                                                  float4* __restrict__ far_acc, int nchunk, int64_t stride) {
   __shared__ float4 s_p[FTILE2];
   __shared__ float4 s_w[FTILE2];
   const int nt = C->n_targets;
-  const int M = C->num_samples;
+  int m0, M;
+  sample_chunk(C->num_samples, nchunk, m0, M);
+  spos += m0;
+  sw += m0;
+  far_acc += blockIdx.y * stride;
   const int tbase = blockIdx.x * FT2 * TT;
   if (tbase >= nt) return;  // uniform per CTA
   float px[TT], py[TT], pz[TT];
@@ -394,11 +406,17 @@ __device__ __forceinline__ void far_fix_one(const dv_params& P, const DevGrid& G
                                             const dv_solver_fields& S, int t, int i, int M, float kden_sum,
                                             uint32_t sk, const int32_t* __restrict__ mult,
                                             const float4* __restrict__ far_acc, const float4* __restrict__ near_v,
-                                            const float* __restrict__ near_S) {
+                                            const float* __restrict__ near_S, int nchunk, int64_t stride) {
   const V3 xi = ldv<D>(F.x, i);
   const float lim = P.far_r2_limit, d2 = P.blob_delta2;
   const float3 bx = make_float3(P.box[0], P.box[1], P.box[2]);
   float4 acc = far_acc[t];
+  for (int k = 1; k < nchunk; ++k) {  // sample-chunk partials, in chunk order
+    const float4 q = far_acc[k * stride + t];
+    acc.x = __fadd_rn(acc.x, q.x);
+    acc.y = __fadd_rn(acc.y, q.y);
+    acc.z = __fadd_rn(acc.z, q.z);
+  }
   int near_cnt = 0;
   int lo0, hi0, lo1, hi1, lo2 = 0, hi2 = 0;
   far_window(P, xi.x, 0, lo0, hi0);
@@ -460,11 +478,12 @@ template <int D, bool BLOB, bool PER>
 __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
                           const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
                           const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
-                          const float4* __restrict__ near_v, const float* __restrict__ near_S) {
+                          const float4* __restrict__ near_v, const float* __restrict__ near_S, int nchunk,
+                          int64_t stride) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= C->n_targets) return;
   far_fix_one<D, BLOB, PER>(P, G, F, S, t, targets[t], C->num_samples, C->kden_sum_f32, 0u, mult, far_acc, near_v,
-                            near_S);
+                            near_S, nchunk, stride);
 }
 
 // scene batch: the target's scene gives M, kden_sum and the key prefix
@@ -479,7 +498,7 @@ __global__ void k_far_fix_b(dv_params P, DevGrid G, dv_fields F, dv_solver_field
   const int i = targets[t];
   const int sc = F.object_id[i];
   far_fix_one<D, BLOB, false>(P, G, F, S, t, i, st[sc].num_samples, st[sc].kden_sum_f32,
-                              (uint32_t)sc << G.scene_shift, mult, far_acc, near_v, near_S);
+                              (uint32_t)sc << G.scene_shift, mult, far_acc, near_v, near_S, 1, 0);
 }
 
 // scene batch main loop: block b is tile b - tile_off_s of the scene s with
@@ -545,20 +564,194 @@ __global__ void __launch_bounds__(FT2) k_far_main_b(dv_params P, const float* __
   }
 }
 
+// ------------------------------------------------ paired-FP32 main loop
+// The reference-kernel main loop with two targets per instruction
+// (Blackwell's sub/mul/fma.rn.f32x2): every lane operation is the scalar
+// loop's own IEEE operation in the same order, so far_acc is bit-identical;
+// the pairs halve the issue slots of a loop that is issue-bound, not
+// FP32-pipe-bound.  Samples are staged in shared memory pre-duplicated
+// ({s, s} pairs, ω̃/kden components negated where the loop subtracts).
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_pack(float a, float b) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2_t v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
+  f2_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+  f2_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// targets [tbase + k·FT2 + tid] (k < TT) of targets[0, nt) against samples
+// [m0, m0 + M); writes far_acc[t] for t < nt.  Block-uniform bounds.
+template <int D, int TT>
+__device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __restrict__ x,
+                                           const int32_t* __restrict__ targets, int nt, int tbase,
+                                           const float4* __restrict__ spos, const float4* __restrict__ sw, int m0,
+                                           int M, float4* __restrict__ far_acc, float4* s4) {
+  constexpr int NP = TT / 2;
+  constexpr int NQ = D == 3 ? 4 : 2;  // duplicated float4 per sample
+  f2_t PX[NP], PY[NP], PZ[NP], AX[NP], AY[NP], AZ[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const int t0 = tbase + (2 * p) * FT2 + threadIdx.x, t1 = tbase + (2 * p + 1) * FT2 + threadIdx.x;
+    const V3 a = ldv<D>(x, targets[t0 < nt ? t0 : nt - 1]);
+    const V3 b = ldv<D>(x, targets[t1 < nt ? t1 : nt - 1]);
+    PX[p] = f2_pack(a.x, b.x);
+    PY[p] = f2_pack(a.y, b.y);
+    PZ[p] = f2_pack(a.z, b.z);
+    AX[p] = AY[p] = AZ[p] = 0ull;
+  }
+  const float lim = P.far_r2_limit;
+  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(s4);
+  for (int base = 0; base < M; base += FTILE2) {
+    const int m = min(FTILE2, M - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += FT2) {
+      const float4 sp = spos[m0 + base + q];
+      const float4 w = sw[m0 + base + q];
+      if (D == 3) {
+        s4[4 * q] = make_float4(sp.x, sp.x, sp.y, sp.y);
+        s4[4 * q + 1] = make_float4(sp.z, sp.z, w.z, w.z);
+        s4[4 * q + 2] = make_float4(-w.z, -w.z, w.y, w.y);
+        s4[4 * q + 3] = make_float4(-w.x, -w.x, 0.0f, 0.0f);
+      } else {
+        s4[2 * q] = make_float4(sp.x, sp.x, sp.y, sp.y);
+        s4[2 * q + 1] = make_float4(w.z, w.z, -w.z, -w.z);
+      }
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int q = 0; q < m; ++q) {
+      const ulonglong2 v0 = s2[NQ * q], v1 = s2[NQ * q + 1];
+      f2_t SZ = 0ull, WZ, NWZ, WY = 0ull, NWX = 0ull;
+      if (D == 3) {
+        const ulonglong2 v2 = s2[NQ * q + 2], v3 = s2[NQ * q + 3];
+        SZ = v1.x;
+        WZ = v1.y;
+        NWZ = v2.x;
+        WY = v2.y;
+        NWX = v3.x;
+      } else {
+        WZ = v1.x;
+        NWZ = v1.y;
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const f2_t DX = f2_sub(PX[p], v0.x), DY = f2_sub(PY[p], v0.y);
+        f2_t R2 = f2_mul(DX, DX);
+        R2 = f2_fma(DY, DY, R2);
+        if (D == 3) {
+          const f2_t DZ = f2_sub(PZ[p], SZ);
+          R2 = f2_fma(DZ, DZ, R2);
+        }
+        float ra, rb;
+        f2_unpack(R2, ra, rb);
+        const f2_t KK = f2_pack(rcp_approx(fmaxf(ra, lim)), rcp_approx(fmaxf(rb, lim)));
+        const f2_t A = f2_mul(KK, DX), B = f2_mul(KK, DY);
+        AX[p] = f2_fma(B, WZ, AX[p]);
+        AY[p] = f2_fma(A, NWZ, AY[p]);
+        if (D == 3) {
+          AZ[p] = f2_fma(A, WY, AZ[p]);
+          AZ[p] = f2_fma(B, NWX, AZ[p]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    float x0, x1, y0, y1, z0, z1;
+    f2_unpack(AX[p], x0, x1);
+    f2_unpack(AY[p], y0, y1);
+    f2_unpack(AZ[p], z0, z1);
+    const int t0 = tbase + (2 * p) * FT2 + threadIdx.x, t1 = tbase + (2 * p + 1) * FT2 + threadIdx.x;
+    if (t0 < nt) far_acc[t0] = make_float4(x0, y0, z0, 0.0f);
+    if (t1 < nt) far_acc[t1] = make_float4(x1, y1, z1, 0.0f);
+  }
+}
+
+template <int D, int TT>
+__global__ void __launch_bounds__(FT2) k_far_main_x2(dv_params P, const float* __restrict__ x,
+                                                     const dv_counters* __restrict__ C,
+                                                     const int32_t* __restrict__ targets,
+                                                     const float4* __restrict__ spos,
+                                                     const float4* __restrict__ sw, float4* __restrict__ far_acc,
+                                                     int nchunk, int64_t stride) {
+  __shared__ float4 s4[(D == 3 ? 4 : 2) * FTILE2];
+  const int nt = C->n_targets;
+  const int tbase = blockIdx.x * FT2 * TT;
+  if (tbase >= nt) return;  // uniform per CTA
+  int m0, M;
+  sample_chunk(C->num_samples, nchunk, m0, M);
+  far_x2_run<D, TT>(P, x, targets, nt, tbase, spos, sw, m0, M, far_acc + blockIdx.y * stride, s4);
+}
+
+template <int D, int TT>
+__global__ void __launch_bounds__(FT2) k_far_main_x2_b(dv_params P, const float* __restrict__ x,
+                                                       const int32_t* __restrict__ targets,
+                                                       const float4* __restrict__ spos,
+                                                       const float4* __restrict__ sw,
+                                                       const dv_scene_state* __restrict__ st, int S,
+                                                       const int32_t* __restrict__ ntiles,
+                                                       float4* __restrict__ far_acc) {
+  __shared__ float4 s4[(D == 3 ? 4 : 2) * FTILE2];
+  const int blk = blockIdx.x;
+  if (blk >= *ntiles) return;  // uniform per CTA
+  int lo = 0, hi = S;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (st[mid].tile_off <= blk)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  const int sc = lo - 1;
+  const int t0 = st[sc].t_start;
+  far_x2_run<D, TT>(P, x, targets + t0, st[sc].n_targets, (blk - st[sc].tile_off) * FT2 * TT, spos, sw,
+                    st[sc].m_off, st[sc].num_samples, far_acc + t0, s4);
+}
+
 template <int D, bool BLOB, bool COMP, bool PER>
 static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const int nb = (int)std::max<int64_t>(1, (nu + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
-#define L(TTV)                                                                                               \
-  k_far_main<D, TTV, BLOB, COMP, PER><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
-                                                                 c->sw, c->far_acc)
+  const dim3 grid(nb, c->far_chunks);
+#define L(TTV)                                                                                                 \
+  k_far_main<D, TTV, BLOB, COMP, PER><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
+                                                                   c->sw, c->far_acc, c->far_chunks, c->cap)
+#define L2(TTV)                                                                                              \
+  k_far_main_x2<D, TTV><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, c->sw,        \
+                                                     c->far_acc, c->far_chunks, c->cap)
+  constexpr bool paired = !BLOB && !COMP && !PER;  // the reference kernel's plain loop
   if (tt <= 2)
     L(2);
-  else if (tt <= 4)
-    L(4);
-  else
-    L(8);
+  else if (tt <= 4) {
+    if (paired)
+      L2(4);
+    else
+      L(4);
+  } else {
+    if (paired)
+      L2(8);
+    else
+      L(8);
+  }
 #undef L
+#undef L2
 }
 
 template <int D, bool PER>
@@ -584,7 +777,7 @@ static void launch_fix(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s)
   const int nb = dv_blocks(std::min<int64_t>(c->n_upper, c->cap), 128);
 #define LF(B, PR)                                                                                      \
   k_far_fix<D, B, PR><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult, \
-                                                 c->far_acc, c->near_v, c->near_S)
+                                                 c->far_acc, c->near_v, c->near_S, c->far_chunks, c->cap)
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   if (c->p.periodic)
     blob ? LF(true, true) : LF(false, true);
@@ -654,28 +847,33 @@ DV_API int dv_autotune(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s,
   DV_CK(c, cudaEventCreate(&e1));
   const int cand[3] = {2, 4, 8};
   float best = 1e30f;
-  int best_t = c->far_tt;
-  for (int tt : cand) {
-    for (int rep = 0; rep < 3; ++rep) {
-      DV_CK(c, cudaEventRecord(e0, c->stream));
-      if (c->p.dim == 2)
-        launch_main<2>(c, f, tt);
-      else
-        launch_main<3>(c, f, tt);
-      DV_LAUNCHED(c);
-      DV_CK(c, cudaEventRecord(e1, c->stream));
-      DV_CK(c, cudaEventSynchronize(e1));
-      float ms = 0.f;
-      DV_CK(c, cudaEventElapsedTime(&ms, e0, e1));
-      if (rep > 0 && ms < best) {
-        best = ms;
-        best_t = tt;
+  int best_t = c->far_tt, best_c = c->far_chunks;
+  for (int nc = 1; nc <= DV_MAX_FAR_CHUNKS; nc += nc < 4 ? 1 : 2) {  // 1, 2, 3, 4, 6, 8
+    c->far_chunks = nc;
+    for (int tt : cand) {
+      for (int rep = 0; rep < 3; ++rep) {
+        DV_CK(c, cudaEventRecord(e0, c->stream));
+        if (c->p.dim == 2)
+          launch_main<2>(c, f, tt);
+        else
+          launch_main<3>(c, f, tt);
+        DV_LAUNCHED(c);
+        DV_CK(c, cudaEventRecord(e1, c->stream));
+        DV_CK(c, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        DV_CK(c, cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0 && ms < best) {
+          best = ms;
+          best_t = tt;
+          best_c = nc;
+        }
       }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->far_tt = best_t;
+  c->far_chunks = best_c;
   if (best_tt) *best_tt = best_t;
   if (best_ms) *best_ms = best;
   return DV_OK;
@@ -686,6 +884,14 @@ DV_API int dv_set_far_tile(dv_ctx* c, int32_t tt) {
   c->far_tt = tt;
   return DV_OK;
 }
+
+DV_API int dv_set_far_chunks(dv_ctx* c, int32_t chunks) {
+  if (!c || chunks < 1 || chunks > DV_MAX_FAR_CHUNKS) return DV_EINVAL;
+  c->far_chunks = chunks;
+  return DV_OK;
+}
+
+DV_API int32_t dv_get_far_chunks(dv_ctx* c) { return c ? c->far_chunks : DV_EINVAL; }
 
 DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   if (!c || !f || !s || !s->sample_idx || !s->kden || !s->d_vort_smoothed)
@@ -759,13 +965,25 @@ static void launch_main_b(dv_ctx* c, const dv_fields* f) {
 #define L(TTV)                                                                                             \
   k_far_main_b<D, TTV, BLOB, COMP><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw,      \
                                                               b->d_state, b->S, b->d_misc, c->far_acc)
+#define L2(TTV)                                                                                            \
+  k_far_main_x2_b<D, TTV><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw, b->d_state,    \
+                                                     b->S, b->d_misc, c->far_acc)
+  constexpr bool paired = !BLOB && !COMP;
   if (c->far_tt <= 2)
     L(2);
-  else if (c->far_tt <= 4)
-    L(4);
-  else
-    L(8);
+  else if (c->far_tt <= 4) {
+    if (paired)
+      L2(4);
+    else
+      L(4);
+  } else {
+    if (paired)
+      L2(8);
+    else
+      L(8);
+  }
 #undef L
+#undef L2
 }
 
 // Scene batch VVPE: the targets are built (dv_build_targets) and the samples

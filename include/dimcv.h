@@ -363,6 +363,12 @@ DV_API int dv_density_error_noalloc(const dv_params* params, const dv_fields* f,
  * FP32-pipe-bound N-body kernels.  Synchronises. */
 DV_API int dv_fp32_peak(dv_ctx* ctx, double* flops_out);
 
+/* Number of sample chunks of the far-field grid (1..8; dv_autotune picks it
+ * with the tile): the main loop runs (target tiles x sample chunks) blocks
+ * and the correction kernel sums the chunk partials in chunk order. */
+DV_API int dv_set_far_chunks(dv_ctx* ctx, int32_t chunks);
+DV_API int32_t dv_get_far_chunks(dv_ctx* ctx);
+
 /* ------------------------------------------------------------------------
  * Differentiable vortex-particle step (2-D).  No reference counterpart: the
  * reference has no derivatives.  The step is the SPH vorticity smoothing

@@ -25,6 +25,7 @@ def lone_run(cfg, grid_num, snap, counts, steps):
     from dimcv_sph_b200.particle_system import ParticleSystem
     ps = ParticleSystem(cfg, grid_num=grid_num)
     sv = ps.build_solver()
+    sv.far_tile = 4  # no autotuning: one sample chunk, as in the batch
     n, nf, ns = counts
     for k, t in snap.items():
         ps.fields[k][:n] = t
