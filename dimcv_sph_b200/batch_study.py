@@ -67,6 +67,7 @@ def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lon
     n_all = sum(s["end"] - s["start"] for s in st)
     ms = _ev_time(b.replay, reps) / 2
     st2 = b.states()
+    eager_same_state = _ev_time(b.step, 2)  # eager steps from the state the graph timing ended in
     out["batch"] = {"ms_per_step": ms, "particle_steps_per_s": n_fluid / (ms * 1e-3),
                     "fluid_particles": n_fluid, "all_particles": n_all,
                     "latency_ms_p50": ms, "latency_ms_p99": ms, "far_tile_targets_per_thread": best,
@@ -74,7 +75,8 @@ def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lon
                     "iters_div_max": max(s["iters_div"] for s in st2),
                     "iters_p_max": max(s["iters_p"] for s in st2),
                     "iters_p_mean": float(np.mean([s["iters_p"] for s in st2])),
-                    "not_converged": sum(1 for s in st2 if s["status"] & 3)}
+                    "scenes_ever_at_iteration_cap": sum(1 for s in st2 if s["status"] & 3),
+                    "eager_ms_per_step_same_state": eager_same_state}
     pairs = float(sum(s["n_targets"] * s["num_samples"] for s in st2))
     out["batch"]["far_pairs_per_step"] = pairs
     sizes = [s["n_fluid"] for s in st2]
