@@ -142,14 +142,27 @@ def dist_setup(args):
     return rank, world, local
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def _all_reduce(x: float, world: int, op: str) -> float:
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    return _all_reduce(x, world, "max")
+
+
+def aggregate_throughput(ms_local: float, units_local: float, world: int):
+    """Whole-job throughput of weakly scaled replicas: the units every rank
+    processed, over the slowest rank's device time.  Returns (ms, units/s)."""
+    ms = _all_reduce(ms_local, world, "max")
+    units = _all_reduce(units_local, world, "sum")
+    return ms, units / (ms * 1e-3)
 
 
 def barrier(world):
@@ -253,9 +266,8 @@ def run_ours(args, rank, world, local):
     lib.dv_profile_read(ctx, C.byref(far_ms), C.byref(far_launches), C.byref(pairs))
     lib.dv_profile(ctx, 0)
     cnt1 = ps.counters()
-    ms = max_over_ranks(ms_local, world)
     n_fluid = 0.5 * (cnt0["n_fluid"] + cnt1["n_fluid"])
-    value = world * n_fluid * args.steps / (ms * 1e-3)
+    ms, value = aggregate_throughput(ms_local, n_fluid * args.steps, world)
 
     # dominant kernel roofline (Monte-Carlo far field, FP32-pipe bound)
     dim = ps.dim

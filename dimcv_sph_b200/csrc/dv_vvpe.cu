@@ -969,9 +969,12 @@ static void launch_main_b(dv_ctx* c, const dv_fields* f) {
   k_far_main_x2_b<D, TTV><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw, b->d_state,    \
                                                      b->S, b->d_misc, c->far_acc)
   constexpr bool paired = !BLOB && !COMP;
-  if (c->far_tt <= 2)
-    L(2);
-  else if (c->far_tt <= 4) {
+  if (c->far_tt <= 2) {
+    if (paired)
+      L2(2);
+    else
+      L(2);
+  } else if (c->far_tt <= 4) {
     if (paired)
       L2(4);
     else

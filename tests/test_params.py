@@ -91,3 +91,27 @@ def test_periodic_box_rejects_bad_shapes():
     # 1/0.12 -> 8 cells of 0.125, 0.5/0.12 -> 4 cells: too few and not the same size
     with pytest.raises(ValueError):
         make_params(SimConfig(config={"Configuration": base}))
+
+
+def test_channel_batch_configs():
+    import math
+    from dimcv_sph_b200.batch import channel_batch_configs, _grid_of
+    cfgs, Ns = channel_batch_configs(n_scenes=64, seed=1)
+    assert len(cfgs) == 64 and Ns.min() >= 2000 and Ns.max() <= 60000
+    # log-uniform: the median of log N sits near the middle of [log 2k, log 60k]
+    mid = 0.5 * (math.log(2000) + math.log(60000))
+    assert abs(float(np.median(np.log(Ns))) - mid) < 0.5
+    grids = np.stack([_grid_of(c) for c in cfgs])
+    for c in cfgs:
+        g = c.get_cfg
+        L, H = g("domainEnd")
+        assert abs(L - 4 * H) < 1e-9
+        u = c.get_fluid_emitters()[0]["velocity"][0]
+        assert 0.5 <= u <= 2.0
+        r = g("cylinderRadius")  # U(0.05, 0.15), capped at a quarter of the height
+        assert r <= 0.15 + 1e-12 and r <= 0.25 * H + 1e-12
+        assert r >= min(0.05, 0.25 * H) - 1e-12
+        assert g("particleRadius") == 0.01 and g("timeStepSize") == 4e-4
+        assert g("computeVis") is False and g("samplerMode") == "inverse_cdf"
+    # the shared batch grid is the largest scene grid
+    assert np.all(grids.max(axis=0) >= grids)
