@@ -76,6 +76,8 @@ PROTOTYPES = {
     "dv_batch_read": (C.c_int, [_P, C.POINTER(DvSceneState), i32, C.POINTER(i64)]),
     "dv_vpm_plan_build": (C.c_int, [_P, _FP, _SP, i32, C.POINTER(DvVpmPlan)]),
     "dv_vpm_smooth": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P]),
+    "dv_vpm_curl": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P]),
+    "dv_vpm_curl_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P]),
     "dv_vpm_smooth_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P]),
     "dv_vpm_velocity": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, i64]),
     "dv_vpm_velocity_bwd": (C.c_int, [_P, C.POINTER(DvVpmPlan), i32, _P, _P, _P, _P, _P, _P, i64]),

@@ -145,6 +145,28 @@ class _Smooth(torch.autograd.Function):
         return gx, gw, None, None, None
 
 
+class _Curl(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, xs, vs, box, plan, xbar):
+        out = torch.empty(xs.shape[0], dtype=xs.dtype, device=xs.device)
+        st = plan.struct(xbar)
+        box._check(box.lib.dv_vpm_curl(box.ctx, C.byref(st), _prec(xs), _ptr(xs), _ptr(vs), _ptr(out)),
+                   "dv_vpm_curl")
+        _save(ctx, box, plan, xbar, xs, vs)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        box, plan, xbar, (xs, vs) = _load(ctx)
+        g = g.contiguous()
+        gv = torch.empty_like(vs)
+        gx = torch.empty_like(xs)
+        st = plan.struct(xbar)
+        box._check(box.lib.dv_vpm_curl_bwd(box.ctx, C.byref(st), _prec(xs), _ptr(xs), _ptr(vs), _ptr(g),
+                                           _ptr(gv), _ptr(gx)), "dv_vpm_curl_bwd")
+        return gx, gv, None, None, None
+
+
 class _Velocity(torch.autograd.Function):
     @staticmethod
     def forward(ctx, xs, wt, box, plan, xbar):
@@ -270,6 +292,15 @@ class VortexBox:
         if plan.xbar is None and getattr(plan, "keep", False):
             plan.xbar = xs.detach().clone()
         return us.index_select(0, plan.inv_perm)
+
+    def curl(self, x: torch.Tensor, v: torch.Tensor, plan: Plan, frozen: bool = False) -> torch.Tensor:
+        """SPH vorticity ω (caller order) of velocities v [n,2] at positions x
+        (compute_vorticity, dimcv_sph.py:228-248), differentiable in x and v."""
+        xs = x.index_select(0, plan.perm)
+        vs = v.index_select(0, plan.perm).contiguous()
+        xbar = plan.xbar.to(xs.dtype).contiguous() if frozen else None
+        ws = _Curl.apply(xs, vs, self, plan, xbar)
+        return ws.index_select(0, plan.inv_perm)
 
     def initial_velocity(self, w: torch.Tensor) -> torch.Tensor:
         """Full Biot-Savart velocity of the initial state (float32, no

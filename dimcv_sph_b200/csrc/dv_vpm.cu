@@ -42,7 +42,7 @@ constexpr int VTS = 128; // sources per shared-memory tile
 template <typename T>
 struct Geo {
   T Lx, Ly, iLx, iLy;  // periodic box and its inverse
-  T invh, kW, c, eps, inv_eps, tiny;
+  T invh, kW, c, eps, inv_eps, tiny, rmin;
 };
 
 template <typename T>
@@ -58,6 +58,7 @@ Geo<T> make_geo(const dv_params& P) {
   g.eps = (T)P.eps;
   g.inv_eps = (T)P.inv_eps;
   g.tiny = sizeof(T) == 4 ? (T)1e-30 : (T)1e-280;
+  g.rmin = (T)P.grad_r_min;
   return g;
 }
 
@@ -122,6 +123,23 @@ __device__ __forceinline__ void w_dw(const Geo<T>& g, T r, T& W, T& dW) {
     const T f = T(1) - q;
     W = T(2) * g.kW * f * f * f;
     dW = T(-6) * g.kW * g.invh * f * f;
+  }
+}
+
+// dW/dr and d²W/dr² of the cubic spline (C² at q = 1/2 and q = 1)
+template <typename T>
+__device__ __forceinline__ void w_d12(const Geo<T>& g, T r, T& d1, T& d2) {
+  const T q = r * g.invh;
+  if (q > T(1)) {
+    d1 = T(0);
+    d2 = T(0);
+  } else if (q <= T(0.5)) {
+    d1 = g.kW * g.invh * (T(6) * q * (T(3) * q - T(2)));
+    d2 = g.kW * g.invh * g.invh * (T(36) * q - T(12));
+  } else {
+    const T f = T(1) - q;
+    d1 = T(-6) * g.kW * g.invh * f * f;
+    d2 = T(12) * g.kW * g.invh * g.invh * f;
   }
 }
 
@@ -197,6 +215,70 @@ __global__ void k_smooth_bwd(Geo<T> g, dv_vpm_plan p, const T* __restrict__ x, c
   gw[i] = a;
   gx[2 * i] = ax;
   gx[2 * i + 1] = ay;
+}
+
+// ------------------------------------------------------------ SPH curl
+// compute_vorticity (dimcv_sph.py:228-248) in 2-D: ω_i = Σ_{j∈N(i)} m_V_j
+// ((v_j − v_i) × ∇W(r_ij))_z with ∇W = W'(|r|) r/|r|, zero for |r| <= 1e-5.
+template <typename T, int IMG>
+__global__ void k_curl(Geo<T> g, dv_vpm_plan p, const T* __restrict__ x, const T* __restrict__ xb,
+                       const T* __restrict__ v, T* __restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
+  const P2<T> vi = ld2(v, i);
+  T acc = T(0);
+  const int k1 = p.nbr_off[i + 1];
+  for (int k = p.nbr_off[i]; k < k1; ++k) {
+    const int j = p.nbr[k];
+    const P2<T> r = rel<T, IMG>(g, x, xb, i, j);
+    const T rn = sqrt(r.x * r.x + r.y * r.y);
+    if (!(rn > g.rmin)) continue;
+    T d1, d2;
+    w_d12<T>(g, rn, d1, d2);
+    const T s = d1 / rn;
+    const P2<T> vj = ld2(v, j);
+    const T ax = vj.x - vi.x, ay = vj.y - vi.y;
+    acc += (T)p.m_V[j] * (ax * (s * r.y) - ay * (s * r.x));
+  }
+  w[i] = acc;
+}
+
+// VJP of k_curl.  With G = ∇W(r_kj), a = v_j − v_k, H = ∂G/∂r:
+//   g_v_k = −Σ_j (g_j m_k + g_k m_j) (G_y, −G_x)
+//   g_x_k =  Σ_j (g_j m_k + g_k m_j) H (−a_y, a_x)
+// H = (W'' − W'/|r|) r̂ r̂ᵀ + (W'/|r|) I (the Hessian of W(|r|), even in r).
+template <typename T, int IMG>
+__global__ void k_curl_bwd(Geo<T> g, dv_vpm_plan p, const T* __restrict__ x, const T* __restrict__ xb,
+                           const T* __restrict__ v, const T* __restrict__ gw, T* __restrict__ gv,
+                           T* __restrict__ gx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= p.n) return;
+  const P2<T> vk = ld2(v, k);
+  const T gk = gw[k], mk = (T)p.m_V[k];
+  T vx = T(0), vy = T(0), xx = T(0), xy = T(0);
+  const int k1 = p.nbr_off[k + 1];
+  for (int e = p.nbr_off[k]; e < k1; ++e) {
+    const int j = p.nbr[e];
+    const P2<T> r = rel<T, IMG>(g, x, xb, k, j);
+    const T rn = sqrt(r.x * r.x + r.y * r.y);
+    if (!(rn > g.rmin)) continue;
+    T d1, d2;
+    w_d12<T>(g, rn, d1, d2);
+    const T sw = gw[j] * mk + gk * (T)p.m_V[j];
+    const T s = d1 / rn;
+    vx -= sw * (s * r.y);
+    vy += sw * (s * r.x);
+    const P2<T> vj = ld2(v, j);
+    const T bx = -(vj.y - vk.y), by = vj.x - vk.x;  // Rᵀ a
+    const T hx = r.x / rn, hy = r.y / rn;
+    const T proj = (d2 - s) * (hx * bx + hy * by);
+    xx += sw * (proj * hx + s * bx);
+    xy += sw * (proj * hy + s * by);
+  }
+  gv[2 * k] = vx;
+  gv[2 * k + 1] = vy;
+  gx[2 * k] = xx;
+  gx[2 * k + 1] = xy;
 }
 
 // ------------------------------------------------------------ velocity
@@ -650,6 +732,26 @@ int smooth_bwd_t(dv_ctx* c, const dv_vpm_plan* p, const void* x, const void* w, 
 }
 
 template <typename T>
+int curl_t(dv_ctx* c, const dv_vpm_plan* p, const void* x, const void* v, void* w) {
+  const Geo<T> g = make_geo<T>(c->p);
+  const T* xb = (const T*)p->xbar;
+  DV_IMG_DISPATCH(img_mode(c, p), (k_curl<T, IMG><<<dv_blocks(p->n), DV_THREADS, 0, c->stream>>>(
+                                       g, *p, (const T*)x, xb, (const T*)v, (T*)w)));
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+template <typename T>
+int curl_bwd_t(dv_ctx* c, const dv_vpm_plan* p, const void* x, const void* v, const void* gw, void* gv, void* gx) {
+  const Geo<T> g = make_geo<T>(c->p);
+  const T* xb = (const T*)p->xbar;
+  DV_IMG_DISPATCH(img_mode(c, p), (k_curl_bwd<T, IMG><<<dv_blocks(p->n), DV_THREADS, 0, c->stream>>>(
+                                       g, *p, (const T*)x, xb, (const T*)v, (const T*)gw, (T*)gv, (T*)gx)));
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+template <typename T>
 int velocity_t(dv_ctx* c, const dv_vpm_plan* p, const void* x, const void* wt, void* u, void* ws,
                int64_t ws_bytes) {
   const Layout L = layout<T>(p->n, p->src_cap, c->num_sms);
@@ -775,4 +877,18 @@ DV_API int dv_vpm_velocity_bwd(dv_ctx* c, const dv_vpm_plan* p, int32_t precisio
   if (!x || !w_s || !g_u || !g_ws || !g_x) return dv_fail(c, DV_EINVAL, "a tensor pointer is NULL");
   return precision == 64 ? velocity_bwd_t<double>(c, p, x, w_s, g_u, g_ws, g_x, ws, ws_bytes)
                          : velocity_bwd_t<float>(c, p, x, w_s, g_u, g_ws, g_x, ws, ws_bytes);
+}
+
+DV_API int dv_vpm_curl(dv_ctx* c, const dv_vpm_plan* p, int32_t precision, const void* x, const void* v, void* w) {
+  if (int rc = check_plan(c, p, precision)) return rc;
+  if (!x || !v || !w) return dv_fail(c, DV_EINVAL, "a tensor pointer is NULL");
+  return precision == 64 ? curl_t<double>(c, p, x, v, w) : curl_t<float>(c, p, x, v, w);
+}
+
+DV_API int dv_vpm_curl_bwd(dv_ctx* c, const dv_vpm_plan* p, int32_t precision, const void* x, const void* v,
+                           const void* g_w, void* g_v, void* g_x) {
+  if (int rc = check_plan(c, p, precision)) return rc;
+  if (!x || !v || !g_w || !g_v || !g_x) return dv_fail(c, DV_EINVAL, "a tensor pointer is NULL");
+  return precision == 64 ? curl_bwd_t<double>(c, p, x, v, g_w, g_v, g_x)
+                         : curl_bwd_t<float>(c, p, x, v, g_w, g_v, g_x);
 }

@@ -418,6 +418,13 @@ DV_API int dv_vpm_smooth(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision
 /* g_w = (∂ω̃/∂ω)^T g_ws, g_x = (∂ω̃/∂x)^T g_ws (written, not accumulated) */
 DV_API int dv_vpm_smooth_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                              const void* w, const void* g_ws, void* g_w, void* g_x);
+/* SPH vorticity of a velocity field (compute_vorticity, dimcv_sph.py:228-248,
+ * 2-D): ω_i = Σ_{j∈N(i)} m_V_j ((v_j − v_i) × ∇W(r_ij))_z; v [n][2]. */
+DV_API int dv_vpm_curl(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x, const void* v,
+                       void* w);
+/* g_v = (∂ω/∂v)^T g_w, g_x = (∂ω/∂x)^T g_w (written, not accumulated) */
+DV_API int dv_vpm_curl_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
+                           const void* v, const void* g_w, void* g_v, void* g_x);
 DV_API int dv_vpm_velocity(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                            const void* w_s, void* u, void* workspace, int64_t workspace_bytes);
 /* g_ws = (∂u/∂ω̃)^T g_u, g_x = (∂u/∂x)^T g_u (written, not accumulated) */

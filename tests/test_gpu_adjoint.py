@@ -156,3 +156,78 @@ def test_mc_gradient_is_unbiased_for_full_biot_savart_gradient(vbox):
     cos16 = float((mean16 * ref).sum() / (mean16.norm() * ref.norm()))
     assert e16 < e1 / 2.5, (e1, e16)
     assert cos16 > 0.6, cos16
+
+
+def test_curl_matches_production_and_fp64_central_differences(vbox):
+    """The SPH curl (ω from v) against the library's fused ∇v/ω sweep, and its
+    VJP in x and v against FP64 central differences."""
+    from dimcv_sph_b200.adjoint import MC
+    box, w0, _ = vbox
+    rng = np.random.default_rng(5)
+    v = torch.from_numpy(rng.normal(0, 0.3, size=(box.n, 2)).astype(np.float32)).to(box.device)
+    plan = box.validate(box.build_plan(box.x0, v, 0, MC))  # runs the production sweep on (x0, v)
+    with torch.no_grad():
+        w32 = box.curl(box.x0, v, plan)
+    perm = plan.perm.long()
+    prod = box.ps.vorticity[: box.n, 2]  # slot order
+    assert nrel(w32.index_select(0, perm).cpu(), prod.cpu()) < 1e-5
+    plan.keep = True
+    x = box.x0.double()
+    with torch.no_grad():
+        box.velocity(x, w0.double(), plan)  # records the nominal positions
+    vd = v.double()
+    g = torch.from_numpy(rng.normal(size=box.n)).to(box.device)
+    xg, vg = x.clone().requires_grad_(True), vd.clone().requires_grad_(True)
+    L = (box.curl(xg, vg, plan, frozen=True) * g).sum()
+    gx, gv = torch.autograd.grad(L, (xg, vg))
+
+    def f(xx, vv):
+        with torch.no_grad():
+            return (box.curl(xx, vv, plan, frozen=True) * g).sum().item()
+
+    ad, fd = [], []
+    for _ in range(32):
+        i, a = int(rng.integers(box.n)), int(rng.integers(2))
+        vp, vm = vd.clone(), vd.clone()
+        vp[i, a] += EPS
+        vm[i, a] -= EPS
+        fd.append((f(x, vp) - f(x, vm)) / (2 * EPS))
+        ad.append(gv[i, a].item())
+        xp, xm = x.clone(), x.clone()
+        xp[i, a] += EPS
+        xm[i, a] -= EPS
+        fd.append((f(xp, vd) - f(xm, vd)) / (2 * EPS))
+        ad.append(gx[i, a].item())
+    assert nrel(ad, fd) < 1e-6, nrel(ad, fd)
+
+
+def test_rollout_from_a_velocity_field(vbox):
+    """ω0 = curl(x0, v0), then an 8-step rollout: the gradient in v0 (curl,
+    smoothing and MC-VVPE adjoints chained) against FP64 central differences."""
+    from dimcv_sph_b200.adjoint import MC
+    box, w0, wt = vbox
+    rng = np.random.default_rng(6)
+    v0 = torch.from_numpy(rng.normal(0, 0.3, size=(box.n, 2))).to(box.device)
+    with torch.no_grad():
+        target = box.rollout(wt.double(), 8)
+        _, plans = box.rollout(w0.double(), 8, mode=MC, keep_plans=True)
+    for p in plans:
+        box.validate(p)
+
+    def loss(v, grad):
+        with torch.set_grad_enabled(grad):
+            w = box.curl(box.x0.double(), v, plans[0], frozen=True)
+            return box.loss(box.rollout(w, 8, plans=plans, frozen=True, checkpoint_every=4), target)
+
+    vg = v0.clone().requires_grad_(True)
+    (g,) = torch.autograd.grad(loss(vg, True), vg)
+    ad, fd = [], []
+    for _ in range(24):
+        i, a = int(rng.integers(box.n)), int(rng.integers(2))
+        vp, vm = v0.clone(), v0.clone()
+        vp[i, a] += EPS
+        vm[i, a] -= EPS
+        fd.append((loss(vp, False).item() - loss(vm, False).item()) / (2 * EPS))
+        ad.append(g[i, a].item())
+    assert np.linalg.norm(fd) > 0
+    assert nrel(ad, fd) < 1e-5, nrel(ad, fd)
