@@ -74,8 +74,8 @@ class SceneBatch:
         from .particle_system import ParticleSystem
         self.cfgs = cfgs
         self.S = S = len(cfgs)
-        if S < 2:
-            raise ValueError("a scene batch needs at least 2 scenes")
+        if S < 1:
+            raise ValueError("a scene batch needs at least one scene")
         self.device = torch.device(device or "cuda")
         self.lib = _lib.load()
         self.grid_num = np.max(np.stack([_grid_of(c) for c in cfgs]), axis=0)

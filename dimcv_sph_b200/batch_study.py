@@ -117,6 +117,34 @@ def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lon
     return out
 
 
+def single_scene_latency(steps: int = 50, warmup: int = 5) -> dict:
+    """The small channel (10k fluid, r = 0.01) stepped alone: the host-driven
+    KarmanVortexSolver.step() against the same scene as a batch of one whose
+    steps replay from a CUDA graph (device emission, device Jacobi loops)."""
+    from . import scenes
+    from .particle_system import ParticleSystem
+    cfg = scenes.channel2d(trim_cylinder=True)
+    cfg.config["Configuration"]["computeVis"] = False
+    ps = ParticleSystem(cfg)
+    sv = ps.build_solver()
+    sv.initialize()
+    for _ in range(warmup):
+        sv.step()
+    lone = _ev_time(sv.step, steps)
+    n_fluid = ps.fluid_particle_num[None]
+    del sv, ps
+    b = SceneBatch([cfg])
+    for _ in range(warmup):
+        b.step()
+    eager = _ev_time(b.step, 10)
+    b.capture(2)
+    b.replay()
+    graph = _ev_time(b.replay, steps // 2) / 2
+    return {"workload": "small channel, 1 scene", "fluid_particles": int(n_fluid),
+            "lone_step_ms": lone, "batch_of_one_eager_ms": eager, "batch_of_one_graph_ms": graph,
+            "graph_speedup_vs_lone": lone / graph}
+
+
 def profile_window(n_scenes: int = 256, seed: int = 0, warmup: int = 6, steps: int = 2, tile: int = 2):
     """Eager batch steps bracketed by cudaProfilerStart/Stop, for a profiler
     started with --profile-from-start off."""
@@ -139,9 +167,13 @@ def main():
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--out", type=str, default=None)
+    ap.add_argument("--single", action="store_true", help="only the one-scene latency comparison")
     ap.add_argument("--profile-window", action="store_true",
                     help="only run 2 eager steps inside cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     a = ap.parse_args()
+    if a.single:
+        print(json.dumps(single_scene_latency()))
+        return
     if a.profile_window:
         st = profile_window(n_scenes=a.scenes)
         print(json.dumps({"profiled_steps": 2, "scenes": len(st)}))

@@ -129,10 +129,12 @@ __global__ void k_batch_ranges(const uint32_t* __restrict__ keys, const dv_count
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = C->n;
   if (p >= n) return;
-  const int s = (int)(keys[p] >> shift);
+  // a batch of one scene has no scene bits in its keys: every active slot is scene 0
+  auto scene = [&](uint32_t k) { return S == 1 ? 0 : (int)(k >> shift); };
+  const int s = scene(keys[p]);
   if (s < 0 || s >= S) return;
-  if (p == 0 || (int)(keys[p - 1] >> shift) != s) st[s].start = p;
-  if (p == n - 1 || (int)(keys[p + 1] >> shift) != s) st[s].end = p + 1;
+  if (p == 0 || scene(keys[p - 1]) != s) st[s].start = p;
+  if (p == n - 1 || scene(keys[p + 1]) != s) st[s].end = p + 1;
 }
 
 // fluid / solid / target counts per scene (one block per scene)

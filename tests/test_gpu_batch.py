@@ -105,3 +105,31 @@ def test_per_scene_bookkeeping(small):
     assert starts[0] == 0 and all(ends[s] == starts[s + 1] for s in range(b.S - 1))
     assert ends[-1] == b.counters()["n"]
     assert st0[0]["emitted"] == 0
+
+
+def test_one_scene_batch_is_the_lone_run_in_a_graph(small):
+    """A batch of one scene (no scene bits in the keys): eager steps equal the
+    lone single-scene run bit for bit, and graph replays equal eager steps."""
+    from dimcv_sph_b200.batch import SceneBatch
+    b = SceneBatch(small[:1], keep_snapshots=True)
+    for _ in range(3):
+        b.step()
+    st = b.states()
+    ps, sv = lone_run(small[0], b.grid_num, b.snaps[0], b.snap_counts[0], 3)
+    c = ps.counters()
+    assert st[0]["start"] == 0 and st[0]["end"] == c["n"]
+    got = b.scene_fields(0, FIELDS, st)
+    for k in FIELDS:
+        assert np.array_equal(got[k], ps.fields[k][: c["n"]].cpu().numpy()), k
+    g = SceneBatch(small[:1])
+    g.step()
+    g.capture(2)
+    g.replay()
+    e = SceneBatch(small[:1])
+    for _ in range(3):
+        e.step()
+    sg, se = g.states(), e.states()
+    assert sg == se
+    fg, fe = g.scene_fields(0, FIELDS, sg), e.scene_fields(0, FIELDS, se)
+    for k in FIELDS:
+        assert np.array_equal(fg[k], fe[k]), k
