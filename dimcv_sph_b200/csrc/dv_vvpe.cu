@@ -298,6 +298,22 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
 
 #define FT2 256
 #define FTILE2 512
+#ifndef DV_FAR_MINB
+// resident CTAs per SM asked of the register allocator for the paired loop
+// (0: none).  Three CTAs cap it at 80 registers: 24 warps per SM instead of
+// 16, which hides more of the rcp -> mul -> fma latency (sphere3d far field
+// 57.5 -> 54.6 ms per step) at the cost of a few dozen bytes of spills.
+#define DV_FAR_MINB 3
+#endif
+#if DV_FAR_MINB > 0
+#define DV_FAR_BOUNDS __launch_bounds__(FT2, DV_FAR_MINB)
+#else
+#define DV_FAR_BOUNDS __launch_bounds__(FT2)
+#endif
+#ifndef DV_FAR_QUNROLL
+#define DV_FAR_QUNROLL 2  // samples per unrolled step of the paired loop
+#endif
+constexpr int kFarQUnroll = DV_FAR_QUNROLL;
 
 // sample chunk blockIdx.y of nchunk: [m0, m0 + M) of the M_total samples;
 // the chunk's partial sums go to far_acc[chunk * stride + t]
@@ -635,7 +651,7 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
       }
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll kFarQUnroll
     for (int q = 0; q < m; ++q) {
       const ulonglong2 v0 = s2[NQ * q], v1 = s2[NQ * q + 1];
       f2_t SZ = 0ull, WZ, NWZ, WY = 0ull, NWX = 0ull;
@@ -685,7 +701,7 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
 }
 
 template <int D, int TT>
-__global__ void __launch_bounds__(FT2) k_far_main_x2(dv_params P, const float* __restrict__ x,
+__global__ void DV_FAR_BOUNDS k_far_main_x2(dv_params P, const float* __restrict__ x,
                                                      const dv_counters* __restrict__ C,
                                                      const int32_t* __restrict__ targets,
                                                      const float4* __restrict__ spos,
@@ -701,7 +717,7 @@ __global__ void __launch_bounds__(FT2) k_far_main_x2(dv_params P, const float* _
 }
 
 template <int D, int TT>
-__global__ void __launch_bounds__(FT2) k_far_main_x2_b(dv_params P, const float* __restrict__ x,
+__global__ void DV_FAR_BOUNDS k_far_main_x2_b(dv_params P, const float* __restrict__ x,
                                                        const int32_t* __restrict__ targets,
                                                        const float4* __restrict__ spos,
                                                        const float4* __restrict__ sw,
