@@ -114,7 +114,8 @@ DV_API void dv_destroy(dv_ctx* c) {
                   c->hist,    c->cell_start, c->cell_end, c->mt[0],     c->mt[1],   c->mt[2],
                   c->scan_part, c->dscan_part, c->red_part, c->ired_part, c->flags, c->offs,
                   c->targets, c->cdf,       c->spos,      c->sw,        c->near_v,  c->near_S,
-                  c->far_acc, c->mult,      c->nbr_off,   c->nbr_idx,   c->d_nbr_ok};
+                  c->far_acc, c->mult,      c->nbr_off,   c->nbr_idx,   c->d_nbr_ok,
+                  c->nbr_rows};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2 * dv_ctx::kProfPool; ++k)
@@ -202,6 +203,10 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   A(c->nbr_off, cap + 1);
   A(c->nbr_idx, c->nbr_cap);
   A(c->d_nbr_ok, 1);
+  // the 3-D build's first pass stores up to 64 neighbours per particle in
+  // fixed rows (a settled lattice has at most 36); 2-D builds have none
+  c->nbr_slots = params->dim == 3 ? 64 : 0;
+  if (c->nbr_slots) A(c->nbr_rows, cap * c->nbr_slots);
   A(c->d_prof, 4);
 #undef A
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_cnt, sizeof(dv_counters));

@@ -269,8 +269,15 @@ __global__ void k_finalize_counts(const int32_t* __restrict__ part, int nparts,
 
 // ------------------------------------------------- per-step neighbour lists
 // After the sort, every sweep of the step visits the same neighbour sets in
-// the same order, so the cell scan (3^d cells, ~8 candidates each in 3-D) is
-// done once here and the sweeps read the lists.  count -> scan -> fill.
+// the same order, so the cell scan (3^d cells) is done once here and the
+// sweeps read the lists as CSR (offsets = exclusive scan of the counts).
+//
+// 3-D (27 cells, ~8 candidates each): one cell-scan pass stores each
+// particle's first `slots` neighbours in its own fixed row and its count; a
+// warp-wide copy then moves the rows into CSR (a particle with more
+// neighbours than slots scans its cells again there).  This saves a second
+// 27-cell scan.  2-D (9 cells): counting is cheap and the fixed rows cost
+// more write traffic than they save, so a count pass and a fill pass.
 template <int D>
 __global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
                             const dv_counters* __restrict__ C, int m, uint32_t* __restrict__ cnt) {
@@ -279,11 +286,6 @@ __global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
   uint32_t k = 0;
   if (i < C->n) for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int, V3, float) { ++k; });
   cnt[i] = k;
-}
-
-__global__ void k_csr_ok(const uint32_t* __restrict__ off, const dv_counters* __restrict__ C, int64_t cap,
-                         int32_t* __restrict__ ok) {
-  *ok = (int64_t)off[C->n] <= cap ? 1 : 0;
 }
 
 template <int D>
@@ -296,24 +298,72 @@ __global__ void k_csr_fill(dv_params P, DevGrid G, const float* __restrict__ x,
   for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) { out[k++] = j; });
 }
 
+template <int D>
+__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x,
+                           const dv_counters* __restrict__ C, int m, int slots, uint32_t* __restrict__ cnt,
+                           int32_t* __restrict__ rows) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  uint32_t k = 0;
+  if (i < C->n) {
+    int32_t* row = rows + (int64_t)i * slots;
+    for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) {
+      if (k < (uint32_t)slots) row[k] = j;
+      ++k;
+    });
+  }
+  cnt[i] = k;
+}
+
+// one warp per group of 32 particles; each row is copied by the whole warp
+// (coalesced reads of the row, coalesced writes of the CSR segment)
+template <int D>
+__global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ x,
+                              const dv_counters* __restrict__ C, int slots, const int32_t* __restrict__ rows,
+                              const uint32_t* __restrict__ off, const int32_t* __restrict__ ok,
+                              int32_t* __restrict__ out) {
+  if (!*ok) return;
+  const int n = C->n;
+  const int lane = threadIdx.x & 31;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31;
+  const int iend = min(i0 + 32, n);
+  for (int i = i0; i < iend; ++i) {
+    const uint32_t k0 = off[i], cnt = off[i + 1] - k0;
+    if (cnt <= (uint32_t)slots) {
+      const int32_t* row = rows + (int64_t)i * slots;
+      for (uint32_t k = lane; k < cnt; k += 32) out[k0 + k] = row[k];
+    } else if (lane == (i & 31)) {
+      uint32_t k = k0;
+      for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) { out[k++] = j; });
+    }
+  }
+}
+
+__global__ void k_csr_ok(const uint32_t* __restrict__ off, const dv_counters* __restrict__ C, int64_t cap,
+                         int32_t* __restrict__ ok) {
+  *ok = (int64_t)off[C->n] <= cap ? 1 : 0;
+}
+
 static int build_csr(dv_ctx* c, const dv_fields* f) {
   const int m = (int)std::min<int64_t>(c->n_upper, c->cap) + 1;
   const int nb = dv_blocks(m);
   DevGrid G = dv_grid_cells(c);
-  if (c->p.dim == 2)
-    k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
+  const bool rows = c->p.dim == 3;
+  if (rows)
+    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->nbr_slots, c->flags,
+                                                    c->nbr_rows);
   else
-    k_csr_count<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
+    k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
   DV_LAUNCHED(c);
   int rc = dv_scan_u32(c, c->flags, c->nbr_off, m);
   if (rc) return rc;
   k_csr_ok<<<1, 1, 0, c->stream>>>(c->nbr_off, c->d_cnt, c->nbr_cap, c->d_nbr_ok);
   DV_LAUNCHED(c);
-  if (c->p.dim == 2)
-    k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
-                                                    c->nbr_idx);
+  if (rows)
+    k_csr_compact<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_slots, c->nbr_rows,
+                                                       c->nbr_off, c->d_nbr_ok, c->nbr_idx);
   else
-    k_csr_fill<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
+    k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
                                                     c->nbr_idx);
   DV_LAUNCHED(c);
   return DV_OK;

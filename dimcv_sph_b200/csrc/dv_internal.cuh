@@ -74,6 +74,8 @@ struct dv_ctx {
   int32_t* nbr_idx = nullptr;   // nbr_cap
   int64_t nbr_cap = 0;
   int32_t* d_nbr_ok = nullptr;  // 1 while the lists match the current positions
+  int32_t* nbr_rows = nullptr;  // 3-D: cap * nbr_slots, the first pass's fixed row of particle i at i * nbr_slots
+  int nbr_slots = 0;
 
   // scene batch (n_scenes > 1): cell keys carry the scene id above
   // scene_shift bits; scene_ptr is the scene id of each slot of the sorted

@@ -296,8 +296,12 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
   }
 }
 
-#define FT2 256
-#define FTILE2 512
+#ifndef FT2
+#define FT2 256  // threads per CTA of the far-field main loops
+#endif
+#ifndef FTILE2
+#define FTILE2 512  // samples staged in shared memory per tile
+#endif
 #ifndef DV_FAR_MINB
 // resident CTAs per SM asked of the register allocator for the paired loop
 // (0: none).  Three CTAs cap it at 80 registers: 24 warps per SM instead of

@@ -166,3 +166,34 @@ def test_sizes_out_of_range_are_errors(cuda):
     p.grid_num[0], p.grid_num[1] = 10, 10
     assert not lib.dv_create(C.byref(p), (1 << 30) + 1, None)
     assert b"capacity" in lib.dv_last_error(None)
+
+
+def test_particle_with_more_neighbours_than_list_slots(cuda):
+    """A crowded 3-D particle (more neighbours than the 64 fixed slots of the
+    list build's first pass) gets its CSR list from a second cell scan; the
+    sweeps stay bit-exact with the oracle."""
+    from dimcv_sph_b200.dimcv_sph import DIMCVSPHSolver
+    from dimcv_sph_b200.particle_system import ParticleSystem
+    from oracle.oracle import OracleSim
+    ps = ParticleSystem(box_cfg(3, reserved=1024))
+    rng = np.random.default_rng(5)
+    spread = rng.uniform(0.05, 0.95, size=(600, 3))
+    cluster = 0.5 + rng.uniform(-0.01, 0.01, size=(80, 3))  # all within h = 0.08 of each other
+    add(ps, np.concatenate([spread, cluster]), rng.normal(0, 0.2, size=(680, 3)))
+    solver = DIMCVSPHSolver(ps)
+    solver.initialize()
+    ps.initialize_particle_system()
+    o = OracleSim(ps.params, ps.particle_max_num, 0)
+    o.load_snapshot(ps.snapshot(), ps.counters())
+    o.counting_sort()
+    assert np.array_equal(o.permutation(), np.arange(o.counters()["n"]))
+    off, _ = o.neighbor_lists()
+    assert np.diff(off).max() > 64
+    for meth, op, field in (("compute_densities", "densities", "density"),
+                            ("compute_DFSPH_factor", "dfsph_factor", "dfsph_factor")):
+        getattr(solver, meth)()
+        o.call(op)
+        assert np.array_equal(ps.snapshot()[field], o.snapshot()[field]), field
+    solver.compute_non_pressure_forces()
+    o.call("nonpressure")
+    assert np.array_equal(ps.snapshot()["acceleration"], o.snapshot()["acceleration"])
