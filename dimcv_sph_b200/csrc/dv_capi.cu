@@ -115,7 +115,7 @@ DV_API void dv_destroy(dv_ctx* c) {
                   c->scan_part, c->dscan_part, c->red_part, c->ired_part, c->flags, c->offs,
                   c->targets, c->cdf,       c->spos,      c->sw,        c->near_v,  c->near_S,
                   c->far_acc, c->mult,      c->nbr_off,   c->nbr_idx,   c->d_nbr_ok,
-                  c->nbr_rows};
+                  c->nbr_rows, c->sflag,   c->srank,     c->sslot};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2 * dv_ctx::kProfPool; ++k)
@@ -197,6 +197,9 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   A(c->near_S, cap);
   A(c->far_acc, cap * DV_MAX_FAR_CHUNKS);
   A(c->mult, cap);
+  A(c->sflag, cap + 1);
+  A(c->srank, cap + 1);
+  A(c->sslot, cap);
   // neighbour lists: 48 (3-D) / 24 (2-D) entries per particle on average,
   // beyond which the sweeps keep scanning cells
   c->nbr_cap = cap * (params->dim == 3 ? 48 : 24);

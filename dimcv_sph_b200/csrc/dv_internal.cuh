@@ -66,6 +66,9 @@ struct dv_ctx {
   float* near_S = nullptr;     // cap
   float4* far_acc = nullptr;   // cap: far-field sums of the main loop, per target
   int32_t* mult = nullptr;     // cap: sample multiplicity per slot
+  uint32_t* sflag = nullptr;   // cap + 1: 1 where mult > 0
+  uint32_t* srank = nullptr;   // cap + 1: exclusive scan of sflag (sampled slots before a slot)
+  int32_t* sslot = nullptr;    // cap: the sampled slots in slot order, srank[j] -> j
   int far_tt = 4;              // targets per thread of the far-field main loop (autotuned)
   int far_chunks = 1;          // sample chunks of the far-field grid (autotuned, <= DV_MAX_FAR_CHUNKS)
 

@@ -391,6 +391,33 @@ __global__ void k_mult(const int32_t* __restrict__ sample_idx, const dv_counters
   }
 }
 
+// The sampled slots in slot order (sslot) and, per slot, the number of
+// sampled slots before it (srank): the samples among the particles
+// [s, e) of a cell are sslot[srank[s] .. srank[e]), in slot order, so the
+// correction kernel reads a cell's few samples instead of testing every
+// particle's multiplicity.
+__global__ void k_sample_flags(const int32_t* __restrict__ mult, int nu, uint32_t* __restrict__ flag) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= nu; j += gridDim.x * blockDim.x)
+    flag[j] = (j < nu && mult[j] > 0) ? 1u : 0u;
+}
+
+__global__ void k_sample_slots(const int32_t* __restrict__ mult, int nu, const uint32_t* __restrict__ rank,
+                               int32_t* __restrict__ slot) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nu; j += gridDim.x * blockDim.x)
+    if (mult[j] > 0) slot[rank[j]] = j;
+}
+
+static int sample_slots(dv_ctx* c) {
+  const int nu = (int)std::min<int64_t>(c->n_upper, c->cap);
+  k_sample_flags<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(c->mult, nu, c->sflag);
+  DV_LAUNCHED(c);
+  int rc = dv_scan_u32(c, c->sflag, c->srank, (int64_t)nu + 1);
+  if (rc) return rc;
+  k_sample_slots<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(c->mult, nu, c->srank, c->sslot);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
 // cell window of a target that contains every particle within h: the 3^d
 // cells around its cell, widened by one cell on a side where the target's
 // cell coordinate is within rounding of a cell face (a particle exactly h
@@ -425,6 +452,7 @@ template <int D, bool BLOB, bool PER>
 __device__ __forceinline__ void far_fix_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
                                             const dv_solver_fields& S, int t, int i, int M, float kden_sum,
                                             uint32_t sk, const int32_t* __restrict__ mult,
+                                            const uint32_t* __restrict__ srank, const int32_t* __restrict__ sslot,
                                             const float4* __restrict__ far_acc, const float4* __restrict__ near_v,
                                             const float* __restrict__ near_S, int nchunk, int64_t stride) {
   const V3 xi = ldv<D>(F.x, i);
@@ -449,9 +477,11 @@ __device__ __forceinline__ void far_fix_one(const dv_params& P, const DevGrid& G
       for (int cc = lo2; cc <= hi2; ++cc) {
         const uint32_t key = (D == 3 ? (kab | __ldg(G.mt2 + wrap_cell(P, cc, 2))) : kab) | sk;
         const int s0 = __ldg(G.start + key), e0 = __ldg(G.end + key);
-        for (int j = s0; j < e0; ++j) {
+        if (s0 >= e0) continue;
+        const uint32_t p1 = __ldg(srank + e0);
+        for (uint32_t p = __ldg(srank + s0); p < p1; ++p) {  // the cell's samples, in slot order
+          const int j = __ldg(sslot + p);
           const int m = mult[j];
-          if (m == 0) continue;
           const V3 xj = ldv<D>(F.x, j);
           if (sqnorm<D>(rel<D>(P, xi, xj)) > lim) continue;  // far: the main loop's term stays
           near_cnt += m;
@@ -497,20 +527,22 @@ __device__ __forceinline__ void far_fix_one(const dv_params& P, const DevGrid& G
 template <int D, bool BLOB, bool PER>
 __global__ void k_far_fix(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
                           const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
-                          const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
+                          const int32_t* __restrict__ mult, const uint32_t* __restrict__ srank,
+                          const int32_t* __restrict__ sslot, const float4* __restrict__ far_acc,
                           const float4* __restrict__ near_v, const float* __restrict__ near_S, int nchunk,
                           int64_t stride) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= C->n_targets) return;
-  far_fix_one<D, BLOB, PER>(P, G, F, S, t, targets[t], C->num_samples, C->kden_sum_f32, 0u, mult, far_acc, near_v,
-                            near_S, nchunk, stride);
+  far_fix_one<D, BLOB, PER>(P, G, F, S, t, targets[t], C->num_samples, C->kden_sum_f32, 0u, mult, srank, sslot,
+                            far_acc, near_v, near_S, nchunk, stride);
 }
 
 // scene batch: the target's scene gives M, kden_sum and the key prefix
 template <int D, bool BLOB>
 __global__ void k_far_fix_b(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
                             const dv_counters* __restrict__ C, const int32_t* __restrict__ targets,
-                            const int32_t* __restrict__ mult, const float4* __restrict__ far_acc,
+                            const int32_t* __restrict__ mult, const uint32_t* __restrict__ srank,
+                            const int32_t* __restrict__ sslot, const float4* __restrict__ far_acc,
                             const float4* __restrict__ near_v, const float* __restrict__ near_S,
                             const dv_scene_state* __restrict__ st) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -518,7 +550,7 @@ __global__ void k_far_fix_b(dv_params P, DevGrid G, dv_fields F, dv_solver_field
   const int i = targets[t];
   const int sc = F.object_id[i];
   far_fix_one<D, BLOB, false>(P, G, F, S, t, i, st[sc].num_samples, st[sc].kden_sum_f32,
-                              (uint32_t)sc << G.scene_shift, mult, far_acc, near_v, near_S, 1, 0);
+                              (uint32_t)sc << G.scene_shift, mult, srank, sslot, far_acc, near_v, near_S, 1, 0);
 }
 
 // scene batch main loop: block b is tile b - tile_off_s of the scene s with
@@ -797,7 +829,8 @@ static void launch_fix(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s)
   const int nb = dv_blocks(std::min<int64_t>(c->n_upper, c->cap), 128);
 #define LF(B, PR)                                                                                      \
   k_far_fix<D, B, PR><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult, \
-                                                 c->far_acc, c->near_v, c->near_S, c->far_chunks, c->cap)
+                                                 c->srank, c->sslot, c->far_acc, c->near_v, c->near_S,    \
+                                                 c->far_chunks, c->cap)
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   if (c->p.periodic)
     blob ? LF(true, true) : LF(false, true);
@@ -936,6 +969,8 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
     DV_CK(c, cudaMemsetAsync(c->mult, 0, sizeof(int32_t) * nu, c->stream));
     k_mult<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(s->sample_idx, c->d_cnt, c->mult);
     DV_LAUNCHED(c);
+    rc = sample_slots(c);
+    if (rc) return rc;
   }
   if (c->prof) {
     if (c->prof_used == dv_ctx::kProfPool) {
@@ -1026,6 +1061,8 @@ int dv_batch_vvpe(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   DV_CK(c, cudaMemsetAsync(c->mult, 0, sizeof(int32_t) * c->cap, c->stream));
   k_mult<<<c->num_sms * 4, DV_THREADS, 0, c->stream>>>(s->sample_idx, c->d_cnt, c->mult);
   DV_LAUNCHED(c);
+  rc = sample_slots(c);
+  if (rc) return rc;
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D, comp = c->p.compensated != 0;
 #define LB(DD)                                                                             \
   if (blob)                                                                                \
@@ -1042,7 +1079,8 @@ int dv_batch_vvpe(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   const int nb = dv_blocks(c->cap, 128);
 #define LF(DD, B)                                                                                         \
   k_far_fix_b<DD, B><<<nb, 128, 0, c->stream>>>(c->p, dv_grid(c), *f, *s, c->d_cnt, c->targets, c->mult,   \
-                                                c->far_acc, c->near_v, c->near_S, b->d_state)
+                                                c->srank, c->sslot, c->far_acc, c->near_v, c->near_S,     \
+                                                b->d_state)
   if (c->p.dim == 2)
     blob ? LF(2, true) : LF(2, false);
   else
