@@ -41,7 +41,7 @@ def _ev_time(fn, reps):
 
 
 def run(n_scenes: int = 256, seed: int = 0, warmup: int = 4, reps: int = 10, lone_rounds: int = 3,
-        tiles=(2, 4, 8)) -> dict:
+        tiles=(2, 4, 6, 8)) -> dict:
     cfgs, Ns = channel_batch_configs(n_scenes=n_scenes, seed=seed)
     t0 = time.perf_counter()
     b = SceneBatch(cfgs)

@@ -302,18 +302,11 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
 #ifndef FTILE2
 #define FTILE2 512  // samples staged in shared memory per tile
 #endif
-#ifndef DV_FAR_MINB
-// resident CTAs per SM asked of the register allocator for the paired loop
-// (0: none).  Three CTAs cap it at 80 registers: 24 warps per SM instead of
-// 16, which hides more of the rcp -> mul -> fma latency (sphere3d far field
-// 57.5 -> 54.6 ms per step) at the cost of a few dozen bytes of spills.
-#define DV_FAR_MINB 3
-#endif
-#if DV_FAR_MINB > 0
-#define DV_FAR_BOUNDS __launch_bounds__(FT2, DV_FAR_MINB)
-#else
-#define DV_FAR_BOUNDS __launch_bounds__(FT2)
-#endif
+// resident CTAs per SM asked of the register allocator for the paired loop:
+// 3 for 2 and 4 targets per thread (80 registers, 24 warps per SM, which hides
+// more of the rcp -> mul -> fma latency than 16: sphere3d far field 57.5 ->
+// 54.6 ms per step), 2 for 6 and 8 (their wider register tiles spill at 80)
+#define DV_FAR_MINB(TT) ((TT) <= 4 ? 3 : 2)
 #ifndef DV_FAR_QUNROLL
 #define DV_FAR_QUNROLL 2  // samples per unrolled step of the paired loop
 #endif
@@ -737,7 +730,7 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
 }
 
 template <int D, int TT>
-__global__ void DV_FAR_BOUNDS k_far_main_x2(dv_params P, const float* __restrict__ x,
+__global__ void __launch_bounds__(FT2, DV_FAR_MINB(TT)) k_far_main_x2(dv_params P, const float* __restrict__ x,
                                                      const dv_counters* __restrict__ C,
                                                      const int32_t* __restrict__ targets,
                                                      const float4* __restrict__ spos,
@@ -753,7 +746,7 @@ __global__ void DV_FAR_BOUNDS k_far_main_x2(dv_params P, const float* __restrict
 }
 
 template <int D, int TT>
-__global__ void DV_FAR_BOUNDS k_far_main_x2_b(dv_params P, const float* __restrict__ x,
+__global__ void __launch_bounds__(FT2, DV_FAR_MINB(TT)) k_far_main_x2_b(dv_params P, const float* __restrict__ x,
                                                        const int32_t* __restrict__ targets,
                                                        const float4* __restrict__ spos,
                                                        const float4* __restrict__ sw,
@@ -777,8 +770,16 @@ __global__ void DV_FAR_BOUNDS k_far_main_x2_b(dv_params P, const float* __restri
                     st[sc].m_off, st[sc].num_samples, far_acc + t0, s4);
 }
 
+// targets per thread actually run for a requested tile: 2, 4 or 8, and 6
+// for the paired loop (the scalar kernels have no 6)
+static inline int far_tile_run(int tt, bool paired) {
+  return tt <= 2 ? 2 : tt <= 4 ? 4 : (tt <= 6 && paired) ? 6 : 8;
+}
+
 template <int D, bool BLOB, bool COMP, bool PER>
-static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
+static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt_req) {
+  constexpr bool paired = !BLOB && !COMP && !PER;  // the reference kernel's plain loop
+  const int tt = far_tile_run(tt_req, paired);
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const int nb = (int)std::max<int64_t>(1, (nu + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
   const dim3 grid(nb, c->far_chunks);
@@ -788,14 +789,15 @@ static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt) {
 #define L2(TTV)                                                                                              \
   k_far_main_x2<D, TTV><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, c->sw,        \
                                                      c->far_acc, c->far_chunks, c->cap)
-  constexpr bool paired = !BLOB && !COMP && !PER;  // the reference kernel's plain loop
-  if (tt <= 2)
+  if (tt == 2)
     L(2);
-  else if (tt <= 4) {
+  else if (tt == 4) {
     if (paired)
       L2(4);
     else
       L(4);
+  } else if (tt == 6) {
+    L2(6);
   } else {
     if (paired)
       L2(8);
@@ -880,7 +882,7 @@ DV_API int dv_profile_read(dv_ctx* c, double* far_ms, int64_t* launches, double*
   return DV_OK;
 }
 
-// Times the far-field main loop for 2, 4 and 8 targets per thread on the
+// Times the far-field main loop for 2, 4, 6 and 8 targets per thread on the
 // current targets and samples (CUDA events, best of two launches after one
 // warm-up) and keeps the fastest for this context.
 DV_API int dv_autotune(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, int32_t* best_tt,
@@ -898,7 +900,7 @@ DV_API int dv_autotune(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s,
   cudaEvent_t e0, e1;
   DV_CK(c, cudaEventCreate(&e0));
   DV_CK(c, cudaEventCreate(&e1));
-  const int cand[3] = {2, 4, 8};
+  const int cand[4] = {2, 4, 6, 8};
   float best = 1e30f;
   int best_t = c->far_tt, best_c = c->far_chunks;
   for (int nc = 1; nc <= DV_MAX_FAR_CHUNKS; nc += nc < 4 ? 1 : 2) {  // 1, 2, 3, 4, 6, 8
@@ -933,7 +935,7 @@ DV_API int dv_autotune(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s,
 }
 
 DV_API int dv_set_far_tile(dv_ctx* c, int32_t tt) {
-  if (!c || (tt != 2 && tt != 4 && tt != 8)) return DV_EINVAL;
+  if (!c || (tt != 2 && tt != 4 && tt != 6 && tt != 8)) return DV_EINVAL;
   c->far_tt = tt;
   return DV_OK;
 }
@@ -1011,7 +1013,11 @@ DV_API int dv_vvpe_mc(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) 
   return DV_OK;
 }
 
-int dv_far_tile_width(const dv_ctx* c) { return FT2 * (c->far_tt <= 2 ? 2 : (c->far_tt <= 4 ? 4 : 8)); }
+static inline bool batch_paired(const dv_ctx* c) {
+  return c->p.kernel_mode != DV_KERNEL_BLOB3D && c->p.compensated == 0;
+}
+
+int dv_far_tile_width(const dv_ctx* c) { return FT2 * far_tile_run(c->far_tt, batch_paired(c)); }
 
 template <int D, bool BLOB, bool COMP>
 static void launch_main_b(dv_ctx* c, const dv_fields* f) {
@@ -1024,16 +1030,19 @@ static void launch_main_b(dv_ctx* c, const dv_fields* f) {
   k_far_main_x2_b<D, TTV><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw, b->d_state,    \
                                                      b->S, b->d_misc, c->far_acc)
   constexpr bool paired = !BLOB && !COMP;
-  if (c->far_tt <= 2) {
+  const int tt = far_tile_run(c->far_tt, paired);  // as dv_far_tile_width, which sized the tiles
+  if (tt == 2) {
     if (paired)
       L2(2);
     else
       L(2);
-  } else if (c->far_tt <= 4) {
+  } else if (tt == 4) {
     if (paired)
       L2(4);
     else
       L(4);
+  } else if (tt == 6) {
+    L2(6);
   } else {
     if (paired)
       L2(8);

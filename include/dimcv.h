@@ -314,10 +314,11 @@ DV_API int dv_sample(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s,
 /* vort2vel (dimcv_sph.py:649-719): near-field neighbour sum, Monte-Carlo
  * far field over sample_idx[0:num_samples], the ‖v_vort‖ < ‖v‖ gate. */
 DV_API int dv_vvpe_mc(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
-/* New (tuning): times the far-field main loop of dv_vvpe_mc for 2, 4 and 8
- * targets per thread on the current targets / samples and keeps the fastest
+/* New (tuning): times the far-field main loop of dv_vvpe_mc for 2, 4, 6 and 8
+ * targets per thread (6 runs as 8 where the loop is not the paired one) and
+ * 1-8 sample chunks on the current targets / samples and keeps the fastest
  * for this context (synchronises; *best_tt / *best_ms may be NULL).
- * dv_set_far_tile sets the choice directly (2, 4 or 8). */
+ * dv_set_far_tile sets the tile directly (2, 4, 6 or 8). */
 DV_API int dv_autotune(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s, int32_t* best_tt,
                        float* best_ms);
 DV_API int dv_set_far_tile(dv_ctx* ctx, int32_t tt);
