@@ -36,6 +36,7 @@ PROTOTYPES = {
     "dv_grid_build": (C.c_int, [_P, _FP, _FP]),
     "dv_get_permutation": (C.c_int, [_P, C.POINTER(i32), i64]),
     "dv_neighbor_lists": (i64, [_P, _FP, _P, _P, i64]),
+    "dv_stored_lists": (i64, [_P, _P, _P, i64]),
     "dv_boundary_volume": (C.c_int, [_P, _FP]),
     "dv_densities": (C.c_int, [_P, _FP]),
     "dv_dfsph_factor": (C.c_int, [_P, _FP]),

@@ -552,6 +552,34 @@ __global__ void k_u32_to_i64(const uint32_t* __restrict__ a, int64_t* __restrict
   if (i < m) b[i] = a[i];
 }
 
+DV_API int64_t dv_stored_lists(dv_ctx* c, uint32_t* dev_offsets, int32_t* dev_nbrs, int64_t max_entries) {
+  if (!c) return DV_EINVAL;
+  dv_counters cnt;
+  int rc = dv_get_counters(c, &cnt);
+  if (rc) return rc;
+  int32_t ok = 0;
+  uint32_t total32 = 0;
+  const int n = cnt.n;
+  DV_CK(c, cudaMemcpyAsync(&ok, c->d_nbr_ok, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  DV_CK(c, cudaMemcpyAsync(&total32, c->nbr_off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  DV_CK(c, cudaStreamSynchronize(c->stream));
+  if (!ok) return dv_fail(c, DV_EINVAL, "dv_stored_lists: no valid lists (positions changed since the grid build)");
+  const int64_t total = total32;
+  if (dev_offsets)
+    DV_CK(c, cudaMemcpyAsync(dev_offsets, c->nbr_off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToDevice,
+                             c->stream));
+  if (dev_nbrs) {
+    if (total > max_entries)
+      return dv_fail(c, DV_ECAPACITY, "dv_stored_lists: %lld entries > max_entries %lld", (long long)total,
+                     (long long)max_entries);
+    if (total > 0)
+      DV_CK(c, cudaMemcpyAsync(dev_nbrs, c->nbr_idx, sizeof(int32_t) * (size_t)total, cudaMemcpyDeviceToDevice,
+                               c->stream));
+  }
+  DV_CK(c, cudaStreamSynchronize(c->stream));
+  return total;
+}
+
 DV_API int64_t dv_neighbor_lists(dv_ctx* c, const dv_fields* f, int64_t* dev_offsets,
                                  int32_t* dev_nbrs, int64_t max_pairs) {
   if (!c || !f || !f->x) return DV_EINVAL;

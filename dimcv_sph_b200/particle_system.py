@@ -311,6 +311,18 @@ class ParticleSystem:
         _lib.check(self.ctx, total, "dv_neighbor_lists")
         return off, nbr[:total]
 
+    def stored_neighbor_lists(self):
+        """The lists the sweeps read, as the last grid build stored them:
+        (offsets int64 [n+1], neighbours int32 [pairs]) on the device."""
+        n = self.particle_num[None]
+        off = torch.zeros(n + 1, dtype=torch.int32, device=self.device)
+        total = self.lib.dv_stored_lists(self.ctx, C.c_void_p(off.data_ptr()), None, 0)
+        _lib.check(self.ctx, total, "dv_stored_lists")
+        nbr = torch.zeros(max(total, 1), dtype=torch.int32, device=self.device)
+        total = self.lib.dv_stored_lists(self.ctx, None, C.c_void_p(nbr.data_ptr()), total)
+        _lib.check(self.ctx, total, "dv_stored_lists")
+        return off.to(torch.int64), nbr[:total]
+
     # ----------------------------------------------------------- counters
     def counters(self) -> dict:
         c = DvCounters()

@@ -250,6 +250,14 @@ DV_API int dv_get_permutation(dv_ctx* ctx, int32_t* host_perm, int64_t n_cap);
  * Synchronises. */
 DV_API int64_t dv_neighbor_lists(dv_ctx* ctx, const dv_fields* f, int64_t* offsets,
                                  int32_t* nbrs, int64_t max_pairs);
+/* New (checking): the neighbour lists the sweeps read, as the last grid build
+ * (dv_grid_build) stored them: CSR offsets (n+1 uint32) and entries in visit
+ * order, copied into device buffers (either may be NULL; call with
+ * nbrs = NULL first to learn the entry count).  Returns the entry count, or a
+ * negative dv_status: DV_EINVAL when no valid lists are stored (positions
+ * or the particle count changed since the build, or they did not fit),
+ * DV_ECAPACITY when max_entries is too small.  Synchronises. */
+DV_API int64_t dv_stored_lists(dv_ctx* ctx, uint32_t* offsets, int32_t* nbrs, int64_t max_entries);
 
 /* ------------------------------------------------------------ SPH / DFSPH */
 /* SPHBase.compute_static_boundary_volume (sph_base.py:91-103). */
