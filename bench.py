@@ -183,6 +183,41 @@ STAGES = {
 }
 
 
+# Algorithmic HBM bytes per particle slot of each stage (3-D; 2-D uses d = 2
+# in the vector terms): every field a stage needs read once and every field
+# it produces written once, neighbour re-reads excluded.  Grid: x, keys and
+# the permuted persistent set (96); DFSPH: densities 21, factor 25, density
+# change 33 (+ 57 + 33 per divergence iteration), non-pressure 41, predict 36,
+# density_adv 33 (+ 57 + 33 per pressure iteration); DIMCV: fused grad-v /
+# curl / KVN / delta-omega 57, smoothing 40, AKDE 20, CDF 12.  The far field is
+# FP32-bound and has its own roofline.
+def stage_bytes(dim: int, it_div: int, it_p: int) -> dict:
+    s = 1.0 if dim == 3 else 2.0 / 3.0  # vector fields shrink with d
+    return {"grid": 96 * s,
+            "dfsph": (21 + 25 + 33 + 90 * it_div + 41 + 36 + 33 + 90 * it_p) * s,
+            "dimcv_sweeps": (57 + 40 + 20 + 12) * s}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def stage_roofline(st: dict, dim: int, slots: int, it_div: int, it_p: int) -> dict:
+    peak, src = hbm_peak()
+    out = {"peak_gbs": peak, "peak_source": src, "unit": "GB/s", "stages": {}}
+    for k, b in stage_bytes(dim, it_div, it_p).items():
+        ms = st.get(k, 0.0)
+        if ms > 0:
+            gbs = b * slots / (ms * 1e-3) / 1e9
+            out["stages"][k] = {"alg_bytes_per_slot": round(b, 1), "achieved": round(gbs, 1),
+                                "frac": round(gbs / peak, 4)}
+    return out
+
+
 def stage_times(solver, ps, steps: int) -> dict:
     """Per-stage device time of `steps` steps (CUDA events on the solver's
     stream around each reference method; outside the timed region)."""
@@ -297,6 +332,8 @@ def run_ours(args, rank, world, local):
     # per-stage device times and HBM fractions (outside the timed region)
     st = stage_times(solver, ps, 3)
     result["stages_ms"] = {k: round(v, 3) for k, v in st.items()}
+    cnt2 = ps.counters()
+    result["stage_roofline"] = stage_roofline(st, dim, cnt2["n"], cnt2["iters_div"], cnt2["iters_p"])
 
     if not args.no_e2e:
         result["e2e"] = e2e(args, ps, solver, world)
