@@ -37,8 +37,8 @@ __global__ void k_vorticity(dv_params P, DevGrid G, dv_fields F, dv_solver_field
   stv<D>(S.v_star, i, vs);
   V3 w{0.f, 0.f, 0.f};
   float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    if (F.material[j] != DV_MATERIAL_FLUID) return;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj != DV_MATERIAL_FLUID) return;
     V3 vj = ldv<D>(F.v, j);
     V3 gw = cubic_gradW<D>(P, r, r2);
     float mv = F.m_V[j];
@@ -71,8 +71,8 @@ __global__ void k_d_vorticity(dv_params P, DevGrid G, dv_fields F, dv_solver_fie
   V3 xi = ldv<D>(F.x, i);
   V3 vsi = ldv<D>(S.v_star, i);
   V3 curl{0.f, 0.f, 0.f};
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    if (F.material[j] != DV_MATERIAL_FLUID) return;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj != DV_MATERIAL_FLUID) return;
     V3 vsj = ldv<D>(S.v_star, j);
     V3 c = cross3(sub3(vsj, vsi), cubic_gradW<D>(P, r, r2));
     float mv = F.m_V[j];
@@ -97,8 +97,8 @@ __global__ void k_smooth(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S
   V3 di = ld4(S.d_vort, i);
   float w0 = cubic_W(P, 0.0f);
   V3 acc{mvi * di.x * w0, mvi * di.y * w0, mvi * di.z * w0};
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3, float r2) {
-    if (F.material[j] != DV_MATERIAL_FLUID) return;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3, float r2, int mj) {
+    if (mj != DV_MATERIAL_FLUID) return;
     float mv = F.m_V[j];
     V3 dj = ld4(S.d_vort, j);
     float wk = cubic_W(P, sqrtf(r2));
@@ -234,8 +234,8 @@ __global__ void k_akde(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
     V3 xi = ldv<D>(F.x, i);
     if (in_vortex_domain<D>(P, xi)) {
       float kd = S.kvn[i] * epan<D>(P, V3{0.f, 0.f, 0.f});
-      for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float) {
-        if (F.material[j] == DV_MATERIAL_FLUID) kd += S.kvn[j] * epan<D>(P, r);
+      for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float, int mj) {
+        if (mj == DV_MATERIAL_FLUID) kd += S.kvn[j] * epan<D>(P, r);
       });
       S.kden[i] = kd;
       contrib = (double)kd;
@@ -378,8 +378,8 @@ __global__ void k_vvpe_near(dv_params P, DevGrid G, dv_fields F, dv_solver_field
   V3 acc{0.f, 0.f, 0.f};
   float Ssum = S.kden[i];
   const bool blob = P.kernel_mode == DV_KERNEL_BLOB3D;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    if (F.material[j] != DV_MATERIAL_FLUID) return;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj != DV_MATERIAL_FLUID) return;
     V3 w = ld4(S.d_vort_smoothed, j);
     if (!blob) {
       V3 rp{r.x, r.y, 0.0f};

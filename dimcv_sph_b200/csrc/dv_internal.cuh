@@ -346,30 +346,39 @@ __device__ __forceinline__ float transit_weight(const dv_params& P, float x0) {
 // in ascending order; j is visited iff j != i and |x_i - x_j| < h, which is
 // tested exactly as r2 < nbr_r2_limit (sqrtf is monotone, so
 // sqrtf(r2) < h  <=>  r2 < the smallest float whose sqrtf reaches h).
-// f(j, r, r2) receives r = x_i - x_j.
-template <int D, typename F>
-__device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevGrid& G,
-                                                  const float* __restrict__ x, int i, V3 xi,
-                                                  F&& f) {
+// f(j, r, r2) receives r = x_i - x_j; for_each_neighbor_m also passes the
+// neighbour's material mj = mat[j], loaded with its index and position one
+// neighbour ahead on the list path (f need not gather it itself).
+template <int D, bool MAT, typename F>
+__device__ __forceinline__ void for_each_neighbor_impl(const dv_params& P, const DevGrid& G,
+                                                       const float* __restrict__ x,
+                                                       const int32_t* __restrict__ mat, int i, V3 xi, F&& f) {
   if (G.nok && __ldg(G.nok)) {  // the lists hold exactly these j, in this order
     uint32_t k = __ldg(G.noff + i);
     const uint32_t k1 = __ldg(G.noff + i + 1);
     if (k >= k1) return;
     // one-deep software pipeline: the next neighbour's index and position
-    // are loaded before f runs on the current one (f still runs in list
-    // order).  Sweeps -5% at 2.37M particles; a two-deep pipeline was slower.
+    // (and material) are loaded before f runs on the current one (f still
+    // runs in list order).  Sweeps -5% at 2.37M particles; a two-deep
+    // pipeline was slower.
     int j = __ldg(G.nidx + k);
     V3 xj = ldv<D>(x, j);
+    int mj = MAT ? __ldg(mat + j) : 0;
 #pragma unroll 1
     while (true) {
       const bool more = ++k < k1;
       const int jn = more ? __ldg(G.nidx + k) : j;
       const V3 xn = ldv<D>(x, jn);
+      const int mn = MAT ? __ldg(mat + jn) : 0;
       V3 r = rel<D>(P, xi, xj);
-      f(j, r, sqnorm<D>(r));
+      if constexpr (MAT)
+        f(j, r, sqnorm<D>(r), mj);
+      else
+        f(j, r, sqnorm<D>(r));
       if (!more) break;
       j = jn;
       xj = xn;
+      mj = mn;
     }
     return;
   }
@@ -403,11 +412,29 @@ __device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevG
           if (j == i) continue;
           V3 r = rel<D>(P, xi, ldv<D>(x, j));
           float r2 = sqnorm<D>(r);
-          if (r2 < lim) f(j, r, r2);
+          if (r2 < lim) {
+            if constexpr (MAT)
+              f(j, r, r2, __ldg(mat + j));
+            else
+              f(j, r, r2);
+          }
         }
       }
     }
   }
+}
+
+template <int D, typename F>
+__device__ __forceinline__ void for_each_neighbor(const dv_params& P, const DevGrid& G,
+                                                  const float* __restrict__ x, int i, V3 xi, F&& f) {
+  for_each_neighbor_impl<D, false>(P, G, x, nullptr, i, xi, f);
+}
+
+template <int D, typename F>
+__device__ __forceinline__ void for_each_neighbor_m(const dv_params& P, const DevGrid& G,
+                                                    const float* __restrict__ x, const int32_t* __restrict__ mat,
+                                                    int i, V3 xi, F&& f) {
+  for_each_neighbor_impl<D, true>(P, G, x, mat, i, xi, f);
 }
 
 // ---------------------------------------------------------------- Philox

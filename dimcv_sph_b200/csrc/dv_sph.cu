@@ -21,8 +21,8 @@ __global__ void k_boundary_volume(dv_params P, DevGrid G, dv_fields F, const dv_
   if (!(F.material[i] == DV_MATERIAL_SOLID && !F.is_dynamic[i])) return;
   V3 xi = ldv<D>(F.x, i);
   float delta = cubic_W(P, 0.0f);
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3, float r2) {
-    if (F.material[j] == DV_MATERIAL_SOLID) delta += cubic_W(P, sqrtf(r2));
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3, float r2, int mj) {
+    if (mj == DV_MATERIAL_SOLID) delta += cubic_W(P, sqrtf(r2));
   });
   F.m_V[i] = 1.0f / delta * 3.0f;
 }
@@ -36,8 +36,7 @@ __global__ void k_densities(dv_params P, DevGrid G, dv_fields F, const dv_counte
   V3 xi = ldv<D>(F.x, i);
   float dens = F.m_V[i] * cubic_W(P, 0.0f);
   float den = 0.0f;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) den += F.m_V[j] * cubic_W(P, sqrtf(r2));
   });
   dens += den;
@@ -54,8 +53,7 @@ __global__ void k_dfsph_factor(dv_params P, DevGrid G, dv_fields F, const dv_cou
   V3 xi = ldv<D>(F.x, i);
   V3 gi{0.f, 0.f, 0.f};
   float sum_k = 0.0f;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID) {
       V3 gw = cubic_gradW<D>(P, r, r2);
       float mm = F.m[j];
@@ -93,8 +91,7 @@ __device__ __forceinline__ double density_change_one(const dv_params& P, const D
   V3 vi = ldv<D>(F.v, i);
   float adv = 0.0f;
   int nn = 0;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
       V3 vj = ldv<D>(F.v, j);
       V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
@@ -133,8 +130,7 @@ __device__ __forceinline__ double density_adv_one(const dv_params& P, const DevG
   V3 xi = ldv<D>(F.x, i);
   V3 vi = ldv<D>(F.v, i);
   float delta = 0.0f;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID) {
       V3 vj = ldv<D>(F.v, j);
       V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
@@ -197,8 +193,7 @@ __device__ __forceinline__ void divergence_iter_one(const dv_params& P, const De
   float k_i = b_i * F.dfsph_factor[i] * F.density[i];
   V3 dv{0.f, 0.f, 0.f};
   const float dt = P.dt;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID) {
       float b_j = F.density_adv[j];
       float k_j = b_j * F.dfsph_factor[j] * F.density[j];
@@ -248,8 +243,7 @@ __device__ __forceinline__ void pressure_iter_one(const dv_params& P, const DevG
   float k_i = b_i * F.dfsph_factor[i];
   const float dt = P.dt;
   const float w = P.has_transit ? transit_weight(P, xi.x) : 1.0f;
-  for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-    int mj = F.material[j];
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
     if (mj == DV_MATERIAL_FLUID) {
       float b_j = F.density_adv[j] - P.density0;
       float k_j = b_j * F.dfsph_factor[j];
@@ -395,8 +389,8 @@ __global__ void k_nonpressure(dv_params P, DevGrid G, dv_fields F, const dv_coun
   if (mi == DV_MATERIAL_FLUID) {
     V3 xi = ldv<D>(F.x, i);
     V3 vi = ldv<D>(F.v, i);
-    for_each_neighbor<D>(P, G, F.x, i, xi, [&](int j, V3 r, float r2) {
-      if (F.material[j] == DV_MATERIAL_FLUID) {
+    for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+      if (mj == DV_MATERIAL_FLUID) {
         V3 vj = ldv<D>(F.v, j);
         V3 dvij{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
         float v_xy = dot<D>(dvij, r);
