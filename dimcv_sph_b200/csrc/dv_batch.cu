@@ -364,8 +364,10 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
   b->mc_fraction = mc_fraction;
   b->stratified = sample_mode == DV_SAMPLE_STRATIFIED;
   b->n_emit = n_emit;
-  // far-field tiles are at least 512 targets wide: sum_s ceil(n_s / 512) <= cap / 512 + S
-  b->cap_tiles = c->cap / 512 + n_scenes + 2;
+  // far-field tiles are at least w = dv_far_min_tile_width() targets wide:
+  // sum_s ceil(n_s / w) <= cap / w + S
+  const int w = dv_far_min_tile_width();
+  b->cap_tiles = c->cap / w + n_scenes + 2;
   b->m_cap = c->cap;
   cudaError_t e = cudaSuccess;
   auto al = [&](void** p, size_t bytes) {

@@ -179,6 +179,7 @@ int dv_batch_draw(dv_ctx* c, const dv_solver_fields* s);
 // dv_vvpe.cu: near field, far field (scene targets x scene samples), gate
 int dv_batch_vvpe(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s);
 int dv_far_tile_width(const dv_ctx* c);
+int dv_far_min_tile_width();  // the narrowest far-field tile (threads per CTA x 2 targets)
 int dv_build_targets(dv_ctx* c, const dv_fields* f);
 
 // ------------------------------------------------------------- scan helpers

@@ -302,11 +302,11 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
 #ifndef FTILE2
 #define FTILE2 512  // samples staged in shared memory per tile
 #endif
-// resident CTAs per SM asked of the register allocator for the paired loop:
-// 3 for 2 and 4 targets per thread (80 registers, 24 warps per SM, which hides
+// resident CTAs per SM asked of the register allocator for the paired loop
+// (for 256-thread CTAs; scaled for other sizes): 3 for 2 and 4 targets per thread (80 registers, 24 warps per SM, which hides
 // more of the rcp -> mul -> fma latency than 16: sphere3d far field 57.5 ->
 // 54.6 ms per step), 2 for 6 and 8 (their wider register tiles spill at 80)
-#define DV_FAR_MINB(TT) ((TT) <= 4 ? 3 : 2)
+#define DV_FAR_MINB(TT) (((TT) <= 4 ? 3 : 2) * (256 / FT2))
 #ifndef DV_FAR_QUNROLL
 #define DV_FAR_QUNROLL 2  // samples per unrolled step of the paired loop
 #endif
@@ -1018,6 +1018,7 @@ static inline bool batch_paired(const dv_ctx* c) {
 }
 
 int dv_far_tile_width(const dv_ctx* c) { return FT2 * far_tile_run(c->far_tt, batch_paired(c)); }
+int dv_far_min_tile_width() { return FT2 * 2; }
 
 template <int D, bool BLOB, bool COMP>
 static void launch_main_b(dv_ctx* c, const dv_fields* f) {
