@@ -12,8 +12,10 @@ Differences a caller can see, all deliberate:
     ``ps.x`` etc. change identity at every rebuild;
   * ``grid_ids`` holds the Morton cell key (the reference stores the
     row-major flat index); neighbour sets are the same;
-  * mesh rigid bodies (trimesh voxelisation) and GGUI buffers are not
-    supported: there is no drawing path and trimesh is not a dependency.
+  * mesh rigid bodies are voxelised by ``mesh.py`` (OBJ / STL, a restatement
+    of trimesh's subdivide voxeliser and hole fill, as trimesh is not a
+    dependency); dynamic ones and GGUI buffers are not supported: there is no
+    two-way coupling and no drawing path.
 """
 from __future__ import annotations
 
@@ -23,6 +25,7 @@ from functools import reduce
 import numpy as np
 import torch
 
+from .mesh import rigid_body_points
 from . import _lib
 from ._abi import MATERIAL_FLUID, MATERIAL_SOLID, DvCounters
 from .fields import particle_fields, solver_fields
@@ -103,9 +106,18 @@ class ParticleSystem:
             self.object_collection[rigid["objectId"]] = rigid
             self.obj_id_rigid_blocks.add(rigid["objectId"])
             rigid_particle_num += n
-        if config.get_rigid_bodies():
-            raise NotImplementedError(
-                "RigidBodies (mesh voxelisation, particle_system.py:616-639) are not supported")
+        # mesh rigid bodies (particle_system.py:90-97, 616-639), static only
+        rigid_bodies = config.get_rigid_bodies() or []
+        for body in rigid_bodies:
+            if body.get("isDynamic"):
+                raise NotImplementedError("dynamic rigid bodies are not supported by this path")
+            if self.dim != 3:
+                raise ValueError("mesh rigid bodies need a 3-D scene")
+            pts = rigid_body_points(body, 2 * g("particleRadius"))
+            body["particleNum"] = int(pts.shape[0])
+            body["voxelizedPoints"] = pts
+            self.object_collection[body["objectId"]] = body
+            rigid_particle_num += int(pts.shape[0])
         self.fluid_emitters = config.get_fluid_emitters()
         self.num_emitters = 0
         for emitter in self.fluid_emitters:
@@ -119,7 +131,7 @@ class ParticleSystem:
             self.particle_max_num += self.reserved_capacity
         if capacity is not None:
             self.particle_max_num = max(int(capacity), self.particle_max_num)
-        self.num_rigid_bodies = len(rigid_blocks)
+        self.num_rigid_bodies = len(rigid_blocks) + len(rigid_bodies)
 
         # device state: two particle field sets (the grid build gathers from one
         # into the other) and the index-stable solver fields
@@ -163,6 +175,16 @@ class ParticleSystem:
                           density=rigid["density"], is_dynamic=rigid["isDynamic"],
                           color=rigid["color"], material=MATERIAL_SOLID,
                           exclude=self._exclusion(rigid))
+        for body in rigid_bodies:  # particle_system.py:276-303
+            self.object_id_rigid_body.add(body["objectId"])
+            n = body["particleNum"]
+            if n == 0:
+                continue
+            pos = np.asarray(body["voxelizedPoints"], np.float32)[:, :self.dim]
+            self.add_particles(body["objectId"], n, pos, np.zeros((n, self.dim), np.float32),
+                               np.full(n, body["density"], np.float32), np.zeros(n, np.float32),
+                               np.full(n, MATERIAL_SOLID, np.int32), np.zeros(n, np.int32),
+                               np.tile(np.asarray(body["color"], np.int32), (n, 1)))
         if verbose:
             print(f"Current particle num: {self.particle_num[None]}, Particle max num: {self.particle_max_num}")
 
