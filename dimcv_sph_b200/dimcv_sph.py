@@ -125,6 +125,7 @@ class DIMCVSPHSolver(SPHBase):
     kinematic_vort_num = property(lambda self: self._sb["kvn"])
     kernel_density = property(lambda self: self._sb["kden"])
     v_vort = property(lambda self: self._sb["v_vort"][:, :3])
+    vorticity_vis = property(lambda self: self._sb["vorticity_vis"][:, :3])
 
     def _set_num_samples(self, value):
         self.injected_num_samples = int(value)
