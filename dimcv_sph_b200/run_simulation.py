@@ -2,9 +2,10 @@
 
     python -m dimcv_sph_b200.run_simulation --scene_file scene.json
 
-Exports PLY frames when the scene sets "exportPLY" (PNG export needs
-matplotlib, which this build does not depend on).  `--max_steps` bounds the
-run; a file named `stop` in the working directory ends it, as in the reference.
+Writes a PNG frame to result_images/ every output interval, and a PLY frame
+to result_ply/ when the scene sets "exportPLY", clearing both folders first.
+`--max_steps` bounds the run; a file named `stop` in the working directory
+ends it, as in the reference.
 """
 from __future__ import annotations
 
@@ -24,6 +25,10 @@ def main(argv=None):
     parser.add_argument("--max_steps", type=int, default=None, help="stop after this many steps")
     parser.add_argument("--device", default="cuda")
     args = parser.parse_args(argv)
+    image_path = Path("result_images")  # run_simulation.py:18-27
+    if image_path.exists():
+        shutil.rmtree(image_path)
+    image_path.mkdir(parents=True, exist_ok=True)
     config = SimConfig(scene_file_path=args.scene_file)
     export_ply = bool(config.get_cfg("exportPLY") or False)
     ply_path = None
@@ -49,6 +54,7 @@ def main(argv=None):
         cnt += 1
         t += solver.dt[None]
         if cnt % output_interval == 0:
+            solver.export_png(cnt_output, image_path)
             if export_ply:
                 solver.export_ply(cnt_output, ply_path)
             cnt_output += 1
