@@ -51,6 +51,7 @@ PROTOTYPES = {
     "dv_nonpressure": (C.c_int, [_P, _FP]),
     "dv_predict_velocity": (C.c_int, [_P, _FP]),
     "dv_advect": (C.c_int, [_P, _FP]),
+    "dv_enforce_boundary": (C.c_int, [_P, _FP, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dv_dimcv_vorticity": (C.c_int, [_P, _FP, _SP]),
     "dv_d_vorticity": (C.c_int, [_P, _FP, _SP]),
     "dv_smooth_d_vort": (C.c_int, [_P, _FP, _SP]),

@@ -686,6 +686,61 @@ DV_API int dv_predict_velocity(dv_ctx* c, const dv_fields* f) {
   return DV_OK;
 }
 
+// enforce_boundary_2D / _3D with simulate_collisions (sph_base.py:118-179,
+// called at karman_vortex.py:226-230): every slot of the capacity whose
+// material is `material` and that is dynamic is clamped into [lo, hi] per
+// axis (a coordinate above hi goes to hi, one at or below lo to lo), and if
+// any axis was clamped its velocity loses (1 + c_f) of its component along
+// the normalised sum of the face normals, c_f = 0.5.
+template <int D>
+__global__ void k_enforce_boundary(dv_fields F, int64_t cap, int material, float lo0, float lo1, float lo2,
+                                   float hi0, float hi1, float hi2) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cap) return;
+  if (!(F.material[i] == material && F.is_dynamic[i])) return;
+  const V3 pos = ldv<D>(F.x, (int)i);
+  V3 x = pos, n{0.f, 0.f, 0.f};
+  const float lo[3] = {lo0, lo1, lo2}, hi[3] = {hi0, hi1, hi2};
+  const float p[3] = {pos.x, pos.y, pos.z};
+  float* xs[3] = {&x.x, &x.y, &x.z};
+  float* ns[3] = {&n.x, &n.y, &n.z};
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    if (p[d] > hi[d]) {
+      *ns[d] += 1.0f;
+      *xs[d] = hi[d];
+    }
+    if (p[d] <= lo[d]) {
+      *ns[d] += -1.0f;
+      *xs[d] = lo[d];
+    }
+  }
+  stv<D>(F.x, (int)i, x);
+  const float len = sqrtf(sqnorm<D>(n));
+  if (len > 1.0e-6f) {
+    const V3 e{n.x / len, n.y / len, D == 3 ? n.z / len : 0.0f};
+    V3 v = ldv<D>(F.v, (int)i);
+    const float s = (1.0f + 0.5f) * dot<D>(v, e);
+    v.x -= s * e.x;
+    v.y -= s * e.y;
+    if (D == 3) v.z -= s * e.z;
+    stv<D>(F.v, (int)i, v);
+  }
+}
+
+DV_API int dv_enforce_boundary(dv_ctx* c, const dv_fields* f, int32_t material, const float* lo, const float* hi) {
+  if (!c || !f || !lo || !hi) return DV_EINVAL;
+  const int nb = dv_blocks(c->cap);
+  if (c->p.dim == 2)
+    k_enforce_boundary<2><<<nb, DV_THREADS, 0, c->stream>>>(*f, c->cap, material, lo[0], lo[1], 0.f, hi[0], hi[1],
+                                                            0.f);
+  else
+    k_enforce_boundary<3><<<nb, DV_THREADS, 0, c->stream>>>(*f, c->cap, material, lo[0], lo[1], lo[2], hi[0], hi[1],
+                                                            hi[2]);
+  DV_LAUNCHED(c);
+  return dv_invalidate_lists(c);  // positions moved
+}
+
 DV_API int dv_advect(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_advect, nblk(c), c->p, *f, c->d_cnt);

@@ -127,6 +127,19 @@ class DIMCVSPHSolver(SPHBase):
     v_vort = property(lambda self: self._sb["v_vort"][:, :3])
     vorticity_vis = property(lambda self: self._sb["vorticity_vis"][:, :3])
 
+    def enforce_boundary_3D(self, particle_type: int):  # sph_base.py:118-179
+        """Clamps the dynamic particles of this material into
+        [padding, domain_size - padding] per axis (bounds in f32, as the
+        reference's kernel constants) and reflects their velocity with loss."""
+        ps = self.ps
+        pad = np.float32(ps.padding)
+        lo = (C.c_float * 3)(*([float(pad)] * 3))
+        hi = (C.c_float * 3)(*[float(np.float32(np.float32(ps.domain_size[d]) - pad)) if d < ps.dim else 0.0
+                               for d in range(3)])
+        self._call("dv_enforce_boundary", int(particle_type), lo, hi)
+
+    enforce_boundary_2D = enforce_boundary_3D
+
     def _set_num_samples(self, value):
         self.injected_num_samples = int(value)
         self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(value))

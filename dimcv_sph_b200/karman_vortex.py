@@ -23,8 +23,7 @@ class KarmanVortexSolver(DIMCVSPHSolver):
         # "cylinder" (x-y distance, the reference) or "sphere" (3-D distance)
         self.obstacle_shape = g("obstacleShape") or "cylinder"
         self.compute_vis = bool(g("computeVis") if g("computeVis") is not None else True)
-        if g("bounceBackBoundary"):
-            raise NotImplementedError("bounceBackBoundary (sph_base.py:118-179) is not supported")
+        self.bounce_back = bool(g("bounceBackBoundary"))
         self.init_cylinder()
 
     def init_cylinder(self):
@@ -58,6 +57,11 @@ class KarmanVortexSolver(DIMCVSPHSolver):
         self.ps.initialize_particle_system()
         self.compute_moving_boundary_volume()
         self.substep()
+        if self.bounce_back:  # karman_vortex.py:226-230
+            if self.ps.dim == 2:
+                self.enforce_boundary_2D(self.ps.material_fluid)
+            else:
+                self.enforce_boundary_3D(self.ps.material_fluid)
 
     def substep(self):  # karman_vortex.py:232-242
         self.compute_densities()

@@ -293,6 +293,13 @@ DV_API int dv_nonpressure(dv_ctx* ctx, const dv_fields* f);
 DV_API int dv_predict_velocity(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.advect (dimcv_sph.py:210-218). */
 DV_API int dv_advect(dv_ctx* ctx, const dv_fields* f);
+/* enforce_boundary_2D / _3D with simulate_collisions (sph_base.py:118-179),
+ * the bounceBackBoundary option of karman_vortex.py:226-230: every slot of the
+ * capacity with this material that is dynamic is clamped into [lo, hi] per
+ * axis (dim floats each; host pointers) and its velocity loses 1.5x its
+ * component along the normalised clamp normal. */
+DV_API int dv_enforce_boundary(dv_ctx* ctx, const dv_fields* f, int32_t material, const float* lo,
+                               const float* hi);
 
 /* --------------------------------------------------------------- DIMCV */
 /* compute_v_star + compute_vorticity + compute_grad_v (dimcv_sph.py:228-293,

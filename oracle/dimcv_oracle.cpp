@@ -845,6 +845,37 @@ DVO_API int dvo_predict_velocity(void* h, dv_fields* f) {  // dimcv_sph.py:220-2
   return 0;
 }
 
+// enforce_boundary_2D / _3D + simulate_collisions (sph_base.py:118-179):
+// all `cap` slots, as the reference's ti.grouped(x) loop over the field
+DVO_API int dvo_enforce_boundary(void* h, dv_fields* f, int material, const float* lo, const float* hi) {
+  Ctx* c = (Ctx*)h;
+  const int D = c->p.dim;
+  for (int64_t i = 0; i < c->cap; ++i) {
+    if (!(f->material[i] == material && f->is_dynamic[i])) continue;
+    const V pos = ldv(*c, f->x, (int)i);
+    V x = pos, n;
+    const float p[3] = {pos.x, pos.y, pos.z};
+    float* xs[3] = {&x.x, &x.y, &x.z};
+    float* ns[3] = {&n.x, &n.y, &n.z};
+    for (int d = 0; d < D; ++d) {
+      if (p[d] > hi[d]) { *ns[d] += 1.0f; *xs[d] = hi[d]; }
+      if (p[d] <= lo[d]) { *ns[d] += -1.0f; *xs[d] = lo[d]; }
+    }
+    stv(*c, f->x, (int)i, x);
+    const float len = std::sqrt(norm_sqr(*c, n));
+    if (len > 1.0e-6f) {
+      const V e{n.x / len, n.y / len, D == 3 ? n.z / len : 0.0f};
+      V v = ldv(*c, f->v, (int)i);
+      const float s = (1.0f + 0.5f) * dotv(*c, v, e);  // c_f = 0.5 (sph_base.py:121)
+      v.x -= s * e.x;
+      v.y -= s * e.y;
+      if (D == 3) v.z -= s * e.z;
+      stv(*c, f->v, (int)i, v);
+    }
+  }
+  return 0;
+}
+
 DVO_API int dvo_advect(void* h, dv_fields* f) {  // dimcv_sph.py:210-218
   Ctx* c = (Ctx*)h;
   const float dt = c->p.dt;

@@ -61,6 +61,7 @@ def load():
             "dvo_sample": (C.c_int, [P, FP, SP, C.c_int, C.c_uint64, C.c_uint64, C.c_int]),
             "dvo_vvpe_mc": (C.c_int, [P, FP, SP, C.c_int]),
             "dvo_bs_full": (C.c_int, [P, FP, P, P, C.c_int, P]),
+            "dvo_enforce_boundary": (C.c_int, [P, FP, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         }
         for name in ("dvo_boundary_volume", "dvo_densities", "dvo_dfsph_factor", "dvo_density_change",
                      "dvo_density_adv", "dvo_divergence_iteration", "dvo_pressure_iteration",
