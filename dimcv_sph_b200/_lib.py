@@ -51,6 +51,8 @@ PROTOTYPES = {
     "dv_nonpressure": (C.c_int, [_P, _FP]),
     "dv_predict_velocity": (C.c_int, [_P, _FP]),
     "dv_advect": (C.c_int, [_P, _FP]),
+    "dv_moving_boundary_volume": (C.c_int, [_P, _FP]),
+    "dv_set_dynamic_rigid": (C.c_int, [_P, C.c_int32]),
     "dv_enforce_boundary": (C.c_int, [_P, _FP, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dv_dimcv_vorticity": (C.c_int, [_P, _FP, _SP]),
     "dv_d_vorticity": (C.c_int, [_P, _FP, _SP]),

@@ -347,6 +347,7 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
     return dv_fail(c, DV_EINVAL, "dv_batch_setup: %d scenes, the context was created for %d", n_scenes,
                    c->p.n_scenes);
   if (c->p.periodic) return dv_fail(c, DV_EUNSUPPORTED, "scene batches of periodic boxes are not built");
+  if (c->dyn_rigid) return dv_fail(c, DV_EUNSUPPORTED, "dynamic rigid particles in a scene batch are not built");
   if (n_emit < 0 || (n_emit > 0 && !emit_pos)) return dv_fail(c, DV_EINVAL, "dv_batch_setup: emitter arrays");
   if (n_scenes > 4096) return dv_fail(c, DV_EINVAL, "dv_batch_setup: at most 4096 scenes");
   int64_t cap_sum = 0;

@@ -71,6 +71,7 @@ struct dv_ctx {
   int32_t* sslot = nullptr;    // cap: the sampled slots in slot order, srank[j] -> j
   int far_tt = 4;              // targets per thread of the far-field main loop (autotuned)
   int far_chunks = 1;          // sample chunks of the far-field grid (autotuned, <= DV_MAX_FAR_CHUNKS)
+  bool dyn_rigid = false;      // dynamic rigid particles present: pressure iterations add their reaction
 
   // per-step neighbour lists (CSR, visit order) built by dv_grid_build
   uint32_t* nbr_off = nullptr;  // cap + 1

@@ -14,11 +14,13 @@
   if (i >= C->n) return;
 
 // --------------------------------------------------------- boundary volume
-// compute_static_boundary_volume (sph_base.py:91-103)
+// compute_static_boundary_volume (sph_base.py:91-103) for the static solids,
+// compute_moving_boundary_volume (:105-112) for the dynamic ones
 template <int D>
-__global__ void k_boundary_volume(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+__global__ void k_boundary_volume(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                  int dynamic) {
   FOR_I;
-  if (!(F.material[i] == DV_MATERIAL_SOLID && !F.is_dynamic[i])) return;
+  if (!(F.material[i] == DV_MATERIAL_SOLID && (F.is_dynamic[i] != 0) == (dynamic != 0))) return;
   V3 xi = ldv<D>(F.x, i);
   float delta = cubic_W(P, 0.0f);
   for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3, float r2, int mj) {
@@ -277,6 +279,42 @@ __device__ __forceinline__ void pressure_iter_one(const dv_params& P, const DevG
   stv<D>(F.v, i, vi);
 }
 
+// The reaction on dynamic rigid particles of one pressure iteration
+// (dimcv_sph.py:540-549): the reference adds, inside the fluid particle's
+// task, -vel_change * inv_dt * rho_fluid / rho_solid to the acceleration of
+// each dynamic solid neighbour, with atomic adds in no fixed order.  Here each
+// dynamic solid gathers the same terms over its fluid neighbours, in its
+// neighbour visit order, after the iteration (which leaves every input of the
+// terms unchanged): the same sum up to the order of its additions, and
+// deterministic.  The divergence solve's reactions (:465-468) are not formed:
+// compute_non_pressure_forces overwrites them with gravity before anything
+// reads them.
+template <int D>
+__global__ void k_rigid_reaction(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                 const int32_t* __restrict__ done) {
+  if (done && *done) return;
+  FOR_I;
+  if (!(F.material[i] == DV_MATERIAL_SOLID && F.is_dynamic[i])) return;
+  const V3 xi = ldv<D>(F.x, i);
+  const float rho_j = F.density[i];
+  const float sm = F.m_V[i] * P.density0;
+  const float dt = P.dt;
+  V3 acc = ldv<D>(F.acceleration, i);
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int q, V3 r, float r2, int mq) {
+    if (mq != DV_MATERIAL_FLUID) return;
+    const float k_q = (F.density_adv[q] - P.density0) * F.dfsph_factor[q];
+    if (!(fabsf(k_q) > P.m_eps)) return;
+    const V3 gw = cubic_gradW<D>(P, V3{-r.x, -r.y, -r.z}, r2);  // at x_q - x_i, as in q's task
+    const float s = -dt * 1.0f * k_q;
+    const V3 vc{s * (sm * gw.x), s * (sm * gw.y), D == 3 ? s * (sm * gw.z) : 0.0f};
+    const float rq = F.density[q];
+    acc.x += -vc.x * P.inv_dt * rq / rho_j;
+    acc.y += -vc.y * P.inv_dt * rq / rho_j;
+    if (D == 3) acc.z += -vc.z * P.inv_dt * rq / rho_j;
+  });
+  stv<D>(F.acceleration, i, acc);
+}
+
 template <int D>
 __global__ void k_divergence_iter(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
                                   const int32_t* __restrict__ done) {
@@ -463,7 +501,20 @@ static inline int nblk(const dv_ctx* c) { return dv_blocks(std::min<int64_t>(c->
 
 DV_API int dv_boundary_volume(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, 0);
+  return DV_OK;
+}
+
+DV_API int dv_moving_boundary_volume(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, 1);
+  return DV_OK;
+}
+
+DV_API int dv_set_dynamic_rigid(dv_ctx* c, int32_t on) {
+  if (!c) return DV_EINVAL;
+  if (on && c->batch) return dv_fail(c, DV_EUNSUPPORTED, "dynamic rigid particles in a scene batch are not built");
+  c->dyn_rigid = on != 0;
   return DV_OK;
 }
 
@@ -521,6 +572,7 @@ DV_API int dv_divergence_iteration(dv_ctx* c, const dv_fields* f) {
 DV_API int dv_pressure_iteration(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_pressure_iter, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
+  if (c->dyn_rigid) LAUNCH_D(k_rigid_reaction, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)nullptr);
   return DV_OK;
 }
 
@@ -544,6 +596,7 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
                  c->red_part);
       } else {
         LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
+        if (c->dyn_rigid) LAUNCH_D(k_rigid_reaction, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
         LAUNCH_D(k_density_adv, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
                  c->red_part);
       }

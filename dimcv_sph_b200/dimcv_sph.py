@@ -60,9 +60,9 @@ class SPHBase:
     def compute_static_boundary_volume(self):  # sph_base.py:91-98
         self._call("dv_boundary_volume")
 
-    def compute_moving_boundary_volume(self):
-        """sph_base.py:105-112: dynamic rigid bodies are not supported, so there
-        is nothing to update."""
+    def compute_moving_boundary_volume(self):  # sph_base.py:105-112
+        if getattr(self.ps, "has_dynamic_rigid", False):
+            self._call("dv_moving_boundary_volume")
 
     def substep(self):
         pass

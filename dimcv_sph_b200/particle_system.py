@@ -14,8 +14,9 @@ Differences a caller can see, all deliberate:
     row-major flat index); neighbour sets are the same;
   * mesh rigid bodies are voxelised by ``mesh.py`` (OBJ / STL, a restatement
     of trimesh's subdivide voxeliser and hole fill, as trimesh is not a
-    dependency); dynamic ones and GGUI buffers are not supported: there is no
-    two-way coupling and no drawing path.
+    dependency); the pressure solve's reaction on dynamic rigid particles is
+    gathered per particle in a fixed order (the reference adds it with
+    unordered atomics); GGUI buffers are not supported: no drawing path.
 """
 from __future__ import annotations
 
@@ -109,8 +110,6 @@ class ParticleSystem:
         # mesh rigid bodies (particle_system.py:90-97, 616-639), static only
         rigid_bodies = config.get_rigid_bodies() or []
         for body in rigid_bodies:
-            if body.get("isDynamic"):
-                raise NotImplementedError("dynamic rigid bodies are not supported by this path")
             if self.dim != 3:
                 raise ValueError("mesh rigid bodies need a 3-D scene")
             pts = rigid_body_points(body, 2 * g("particleRadius"))
@@ -168,8 +167,6 @@ class ParticleSystem:
             start = np.array(rigid["start"]) + offset
             end = np.array(rigid["end"]) + offset
             scale = np.array(rigid["scale"])
-            if rigid.get("isDynamic"):
-                raise NotImplementedError("dynamic rigid blocks are not supported by this path")
             self.add_cube(object_id=rigid["objectId"], lower_corner=start,
                           cube_size=(end - start) * scale, velocity=rigid["velocity"],
                           density=rigid["density"], is_dynamic=rigid["isDynamic"],
@@ -180,11 +177,19 @@ class ParticleSystem:
             n = body["particleNum"]
             if n == 0:
                 continue
+            dyn = 1 if body.get("isDynamic") else 0
+            vel = np.asarray(body["velocity"], np.float32)[:self.dim] if dyn else np.zeros(self.dim, np.float32)
             pos = np.asarray(body["voxelizedPoints"], np.float32)[:, :self.dim]
-            self.add_particles(body["objectId"], n, pos, np.zeros((n, self.dim), np.float32),
+            self.add_particles(body["objectId"], n, pos, np.tile(vel, (n, 1)),
                                np.full(n, body["density"], np.float32), np.zeros(n, np.float32),
-                               np.full(n, MATERIAL_SOLID, np.int32), np.zeros(n, np.int32),
+                               np.full(n, MATERIAL_SOLID, np.int32), np.full(n, dyn, np.int32),
                                np.tile(np.asarray(body["color"], np.int32), (n, 1)))
+        # dynamic rigid particles (rigid blocks or bodies with isDynamic): no
+        # shape matching, as in the reference, where it is never called; the
+        # pressure solve adds their reaction (dimcv_sph.py:540-549)
+        self.has_dynamic_rigid = any(bool(r.get("isDynamic")) for r in list(rigid_blocks) + list(rigid_bodies))
+        if self.has_dynamic_rigid:
+            _lib.check(self.ctx, self.lib.dv_set_dynamic_rigid(self.ctx, 1), "dv_set_dynamic_rigid")
         if verbose:
             print(f"Current particle num: {self.particle_num[None]}, Particle max num: {self.particle_max_num}")
 

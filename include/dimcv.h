@@ -262,6 +262,15 @@ DV_API int64_t dv_stored_lists(dv_ctx* ctx, uint32_t* offsets, int32_t* nbrs, in
 /* ------------------------------------------------------------ SPH / DFSPH */
 /* SPHBase.compute_static_boundary_volume (sph_base.py:91-103). */
 DV_API int dv_boundary_volume(dv_ctx* ctx, const dv_fields* f);
+/* compute_moving_boundary_volume (sph_base.py:105-112): the same volume for
+ * the dynamic solids, once per step. */
+DV_API int dv_moving_boundary_volume(dv_ctx* ctx, const dv_fields* f);
+/* New (switch): the scene has dynamic rigid particles.  While on, every
+ * pressure iteration (dv_pressure_iteration, dv_pressure_solve) also forms
+ * the reaction on them (dimcv_sph.py:540-549), gathered per solid in its
+ * neighbour order instead of the reference's unordered atomic adds.  Not
+ * available in a scene batch. */
+DV_API int dv_set_dynamic_rigid(dv_ctx* ctx, int32_t on);
 /* DIMCVSPHSolver.compute_densities (dimcv_sph.py:126-148). */
 DV_API int dv_densities(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.compute_DFSPH_factor (dimcv_sph.py:86-124). */

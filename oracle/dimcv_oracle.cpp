@@ -50,6 +50,7 @@ struct Ctx {
   // (neighbours are still read everywhere); fixed Jacobi iteration counts
   int lo = 0, hi = 0x7fffffff;
   int fixed_div = 0, fixed_p = 0;
+  bool dyn_rigid = false;  // pressure iterations add the reaction on dynamic solids
 };
 
 inline int range_lo(const Ctx* c) { return std::max(0, c->lo); }
@@ -514,12 +515,14 @@ DVO_API int64_t dvo_neighbor_lists(void* h, const dv_fields* f, int64_t* off, in
 
 // ------------------------------------------------------------------- SPH
 // compute_static_boundary_volume (sph_base.py:91-103)
-DVO_API int dvo_boundary_volume(void* h, dv_fields* f) {
+// compute_static_boundary_volume (sph_base.py:91-98) and, for the dynamic
+// solids, compute_moving_boundary_volume (:105-112)
+static int boundary_volume(void* h, dv_fields* f, bool dynamic) {
   Ctx* c = (Ctx*)h;
   const dv_params& P = c->p;
 #pragma omp parallel for schedule(static)
   for (int i = range_lo(c); i < range_hi(c); ++i) {
-    if (!(f->material[i] == DV_MATERIAL_SOLID && !f->is_dynamic[i])) continue;
+    if (!(f->material[i] == DV_MATERIAL_SOLID && (f->is_dynamic[i] != 0) == dynamic)) continue;
     float delta = cubic_kernel(P, 0.0f);
     V xi = ldv(*c, f->x, i);
     for_all_neighbors(*c, f->x, i, [&](int j, V) {
@@ -532,6 +535,39 @@ DVO_API int dvo_boundary_volume(void* h, dv_fields* f) {
     f->m_V[i] = 1.0f / delta * 3.0f;
   }
   return 0;
+}
+
+DVO_API int dvo_boundary_volume(void* h, dv_fields* f) { return boundary_volume(h, f, false); }
+DVO_API int dvo_moving_boundary_volume(void* h, dv_fields* f) { return boundary_volume(h, f, true); }
+DVO_API void dvo_set_dynamic_rigid(void* h, int on) { ((Ctx*)h)->dyn_rigid = on != 0; }
+
+// the reaction of one pressure iteration on the dynamic solids
+// (dimcv_sph.py:540-549): -vel_change * inv_dt * rho_fluid / rho_solid from
+// every fluid neighbour, gathered per solid in its neighbour visit order
+static void rigid_reaction(Ctx* c, dv_fields* f) {
+  const dv_params& P = c->p;
+  const float dt = P.dt;
+#pragma omp parallel for schedule(static)
+  for (int i = range_lo(c); i < range_hi(c); ++i) {
+    if (!(f->material[i] == DV_MATERIAL_SOLID && f->is_dynamic[i])) continue;
+    const float rho_j = f->density[i];
+    const float s = f->m_V[i] * P.density0;
+    V acc = ldv(*c, f->acceleration, i);
+    for_all_neighbors(*c, f->x, i, [&](int q, V r) {  // r = x_i - x_q
+      if (f->material[q] != DV_MATERIAL_FLUID) return;
+      const float k_q = (f->density_adv[q] - P.density0) * f->dfsph_factor[q];
+      if (!(std::fabs(k_q) > P.m_eps)) return;
+      V g = cubic_kernel_derivative(*c, V{-r.x, -r.y, -r.z});  // at x_q - x_i, as in q's task
+      V gp{s * g.x, s * g.y, s * g.z};
+      const float vc0 = -dt * 1.0f * k_q;
+      V vc{vc0 * gp.x, vc0 * gp.y, vc0 * gp.z};
+      const float rq = f->density[q];
+      acc.x += -vc.x * P.inv_dt * rq / rho_j;
+      acc.y += -vc.y * P.inv_dt * rq / rho_j;
+      acc.z += -vc.z * P.inv_dt * rq / rho_j;
+    });
+    stv(*c, f->acceleration, i, acc);
+  }
 }
 
 // compute_densities (dimcv_sph.py:126-148)
@@ -745,6 +781,7 @@ DVO_API int dvo_pressure_iteration(void* h, dv_fields* f) {
     });
     stv(*c, f->v, i, vi);
   }
+  if (c->dyn_rigid) rigid_reaction(c, f);
   return 0;
 }
 

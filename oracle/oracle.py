@@ -62,10 +62,12 @@ def load():
             "dvo_vvpe_mc": (C.c_int, [P, FP, SP, C.c_int]),
             "dvo_bs_full": (C.c_int, [P, FP, P, P, C.c_int, P]),
             "dvo_enforce_boundary": (C.c_int, [P, FP, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+            "dvo_set_dynamic_rigid": (None, [P, C.c_int]),
         }
         for name in ("dvo_boundary_volume", "dvo_densities", "dvo_dfsph_factor", "dvo_density_change",
                      "dvo_density_adv", "dvo_divergence_iteration", "dvo_pressure_iteration",
-                     "dvo_nonpressure", "dvo_predict_velocity", "dvo_advect", "dvo_life_time"):
+                     "dvo_nonpressure", "dvo_predict_velocity", "dvo_advect", "dvo_life_time",
+                     "dvo_moving_boundary_volume"):
             sig[name] = (C.c_int, [P, FP])
         for name in ("dvo_dimcv_vorticity", "dvo_d_vorticity", "dvo_smooth_d_vort", "dvo_record_samples",
                      "dvo_akde", "dvo_vis"):

@@ -117,16 +117,3 @@ def test_sphere_voxelisation_is_bounded_and_filled():
     key = {tuple(np.round(p / pitch).astype(int)) for p in pts}
     assert all(tuple(np.round(p / pitch).astype(int)) in key for p in inside)
 
-
-def test_dynamic_mesh_rigid_body_is_rejected(tmp_path):
-    from dimcv_sph_b200.config_builder import SimConfig
-    from dimcv_sph_b200.particle_system import ParticleSystem
-    p = tmp_path / "box.obj"
-    write_obj(p, BOX_V, BOX_F)
-    cfg = SimConfig(config={
-        "Configuration": {"domainStart": [0.0, 0.0, 0.0], "domainEnd": [1.0, 1.0, 1.0], "particleRadius": 0.02,
-                          "density0": 1000, "timeStepSize": 1e-3},
-        "RigidBodies": [{"objectId": 3, "geometryFile": str(p), "isDynamic": True, "density": 1000.0,
-                         "color": [0, 0, 0], "velocity": [0.0, 0.0, 0.0]}]})
-    with pytest.raises(NotImplementedError):
-        ParticleSystem(cfg)
