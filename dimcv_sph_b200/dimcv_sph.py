@@ -67,10 +67,28 @@ class SPHBase:
     def substep(self):
         pass
 
+    def enforce_boundary_3D(self, particle_type: int):  # sph_base.py:118-179
+        """Clamps the dynamic particles of this material into
+        [padding, domain_size - padding] per axis (bounds in f32, as the
+        reference's kernel constants) and reflects their velocity with loss."""
+        ps = self.ps
+        pad = np.float32(ps.padding)
+        lo = (C.c_float * 3)(*([float(pad)] * 3))
+        hi = (C.c_float * 3)(*[float(np.float32(np.float32(ps.domain_size[d]) - pad)) if d < ps.dim else 0.0
+                               for d in range(3)])
+        self._call("dv_enforce_boundary", int(particle_type), lo, hi)
+
+    enforce_boundary_2D = enforce_boundary_3D
+
     def step(self):  # sph_base.py:224-232
         self.ps.initialize_particle_system()
         self.compute_moving_boundary_volume()
         self.substep()
+        if self.ps.cfg.get_cfg("bounceBackBoundary"):
+            if self.ps.dim == 2:
+                self.enforce_boundary_2D(self.ps.material_fluid)
+            else:
+                self.enforce_boundary_3D(self.ps.material_fluid)
 
 
 class DIMCVSPHSolver(SPHBase):
@@ -126,19 +144,6 @@ class DIMCVSPHSolver(SPHBase):
     kernel_density = property(lambda self: self._sb["kden"])
     v_vort = property(lambda self: self._sb["v_vort"][:, :3])
     vorticity_vis = property(lambda self: self._sb["vorticity_vis"][:, :3])
-
-    def enforce_boundary_3D(self, particle_type: int):  # sph_base.py:118-179
-        """Clamps the dynamic particles of this material into
-        [padding, domain_size - padding] per axis (bounds in f32, as the
-        reference's kernel constants) and reflects their velocity with loss."""
-        ps = self.ps
-        pad = np.float32(ps.padding)
-        lo = (C.c_float * 3)(*([float(pad)] * 3))
-        hi = (C.c_float * 3)(*[float(np.float32(np.float32(ps.domain_size[d]) - pad)) if d < ps.dim else 0.0
-                               for d in range(3)])
-        self._call("dv_enforce_boundary", int(particle_type), lo, hi)
-
-    enforce_boundary_2D = enforce_boundary_3D
 
     def _set_num_samples(self, value):
         self.injected_num_samples = int(value)
