@@ -1,19 +1,20 @@
 // Allocation-free variant of the FP64 density-error reduction
-// (dv_density_error), for callers that must not allocate device memory: code
-// that runs while a stream is being captured in the global capture mode
-// (cudaMalloc fails there), real-time step loops that forbid allocation after
-// start-up, and host frameworks whose own allocator owns all device memory.
+// (dv_density_error), for callers that must not allocate device memory:
+// real-time step loops that forbid allocation after start-up, and host
+// frameworks whose own allocator owns all device memory.  It avoids
+// allocation only: it copies its result to the host and synchronises the
+// stream, so it is not made on a stream that is being captured.
 //
 // The scratch (one FP64 partial per 256-particle block plus the result) lives
 // in a file-scope __device__ array, so every GPU that loads this library holds
 // its 512 KB until the process exits.  In host code the array's name is only
-// a host-side stand-in, so its device address is fetched once per device with
-// cudaGetSymbolAddress and cached.  Every call shares the array: calls that
-// overlap on the GPU (different streams, or different host threads on one
-// device) race on it.  Each call writes every partial it reads, so nothing
-// has to start at zero.
-#include <mutex>
-
+// a host-side stand-in, so its device address is fetched with
+// cudaGetSymbolAddress on every call, with the caller's device current (a
+// lookup in the loaded module, not an allocation); a cached address could
+// point at freed memory after a device reset.  Every call shares the array:
+// calls that overlap on the GPU (different streams, or different host
+// threads on one device) race on it.  Each call writes every partial it
+// reads, so nothing has to start at zero.
 #include "dv_internal.cuh"
 
 #define DV_NOALLOC_BLOCK 256
@@ -23,9 +24,6 @@
 static __device__ __align__(256) double g_dv_noalloc_scratch[DV_NOALLOC_MAX_BLOCKS + 32];
 
 namespace {
-std::mutex g_noalloc_mu;
-double* g_noalloc_dev[1024] = {};  // device address of the scratch, per device ordinal
-
 // block partials of compute_density_error (dimcv_sph.py:407-419) over slots
 // [0, n); the same per-block layout and term as k_density_error in dv_sph.cu
 template <int D>
@@ -70,21 +68,10 @@ DV_API int dv_density_error_noalloc(const dv_params* params, const dv_fields* f,
                    (long long)DV_NOALLOC_MAX_N);
   if (n > 0 && (!f->material || !f->density_adv || (params->has_transit && !f->x)))
     return dv_fail(nullptr, DV_EINVAL, "dv_density_error_noalloc: a needed field pointer is NULL");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return dv_cuda_check(nullptr, e, "cudaGetDevice");
-  if (dev < 0 || dev >= 1024) return dv_fail(nullptr, DV_EINVAL, "device ordinal %d out of range", dev);
-  double* scratch;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_dev[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_dv_noalloc_scratch);
-      if (e != cudaSuccess) return dv_cuda_check(nullptr, e, "cudaGetSymbolAddress(noalloc scratch)");
-      g_noalloc_dev[dev] = static_cast<double*>(p);
-    }
-    scratch = g_noalloc_dev[dev];
-  }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_dv_noalloc_scratch);
+  if (e != cudaSuccess) return dv_cuda_check(nullptr, e, "cudaGetSymbolAddress(noalloc scratch)");
+  double* scratch = static_cast<double*>(p);
   cudaStream_t s = (cudaStream_t)stream;
   const int nb = n > 0 ? (int)((n + DV_NOALLOC_BLOCK - 1) / DV_NOALLOC_BLOCK) : 1;
   double* result = scratch + DV_NOALLOC_MAX_BLOCKS;

@@ -367,19 +367,22 @@ DV_API int dv_profile(dv_ctx* ctx, int32_t enable);
 DV_API int dv_profile_read(dv_ctx* ctx, double* far_ms, int64_t* launches, double* pairs);
 
 /* Allocation-free FP64 density error, for callers that cannot allocate
- * device memory: a stream being captured in the global capture mode (where
- * cudaMalloc fails), real-time loops that forbid allocation after start-up,
- * or hosts whose allocator owns all device memory.  No counterpart in the
- * reference; it computes what dv_density_error computes (the reference's
+ * device memory: real-time step loops that forbid allocation after
+ * start-up, and hosts whose own allocator owns all device memory (a pool
+ * that reserved the GPU, or an embedding application that hands this
+ * library only device pointers).  No counterpart in the reference; it
+ * computes what dv_density_error computes (the reference's
  * compute_density_error sum, in FP64) without a context: no dv_create, no
  * cudaMalloc / cudaFree.  Its scratch is a 512 KB file-scope __device__
  * array that every GPU loading the library keeps until exit.  Limit: n <=
- * 16,777,216 particles (larger n returns DV_ECAPACITY).  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race.  Fields are device pointers of slots [0, n);
- * *out (host) receives the sum; synchronises `stream`.  Errors: negative
- * dv_status, message via dv_last_error(NULL). */
+ * 16,777,216 particles (larger n returns DV_ECAPACITY).  Each call looks up
+ * the array's device address on the current device (cudaGetSymbolAddress),
+ * so the address stays right after a device reset.  The call copies the
+ * sum to the host and synchronises `stream`, so it cannot be made on a
+ * stream that is being captured into a CUDA graph: it avoids allocation,
+ * nothing more.  All calls share the array: calls that overlap on the GPU
+ * race.  Fields are device pointers of slots [0, n); *out (host) receives
+ * the sum.  Errors: negative dv_status, message via dv_last_error(NULL). */
 DV_API int dv_density_error_noalloc(const dv_params* params, const dv_fields* f, int32_t n,
                                     float offset, double* out, void* stream);
 

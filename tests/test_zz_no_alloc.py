@@ -1,13 +1,16 @@
 """dv_density_error_noalloc: the allocation-free density-error reduction.
 
-Some callers cannot allocate device memory: a stream captured in the global
-capture mode (cudaMalloc fails there), real-time step loops that forbid
-allocation after start-up, or hosts whose allocator owns all device memory.
-This entry point needs no context and no cudaMalloc; its scratch is a fixed
-file-scope device array.  The test calls it through the C ABI twice in a row
-and checks both results against the context-based dv_density_error on the
-same fields, within 1e-12 relative (both are FP64 sums of the same f32 terms
-in the same fixed order, so they agree exactly in practice).
+Some callers cannot allocate device memory: real-time step loops that forbid
+allocation once they run, and hosts whose own allocator owns all device
+memory and hand this library only device pointers.  This entry point needs
+no context and no cudaMalloc; its scratch is a fixed file-scope device array.
+It still copies its result to the host and synchronises the stream, so it is
+not used on a stream that is being captured.  The test calls it through the
+C ABI twice in a row and checks both results against the context-based
+dv_density_error on the same fields, within 1e-12 relative (both are FP64
+sums of the same f32 terms in the same fixed order, so they agree exactly in
+practice).  The scenes cover 2-D with and without the divergence transit
+weight and the 3-D sphere scene; an empty range must give exactly 0.
 
 This file sorts last on purpose: a failure here stops a `-x` run only after
 every other test has run.
@@ -24,16 +27,22 @@ pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
 
+SCENES = {
+    "channel2d_transit": lambda: scenes.channel2d(length=2.0, reserved=200, transit=True),
+    "channel2d_plain": lambda: scenes.channel2d(length=2.0, reserved=200, transit=False),
+    "sphere3d_coarse": lambda: scenes.sphere3d(radius=0.016, dt=6.4e-4),
+}
 
-def _scene():
+
+def _scene(name="channel2d_transit"):
     from dimcv_sph_b200.particle_system import ParticleSystem
-    ps = ParticleSystem(scenes.channel2d(length=2.0, reserved=200))
+    ps = ParticleSystem(SCENES[name]())
     solver = ps.build_solver()
     n = ps.particle_num[None]
     # a seeded velocity disturbance so that the density change is not zero
     rng = np.random.default_rng(1)
     fl = ps.material[:n] == 1
-    noise = torch.from_numpy(rng.normal(0, 0.3, size=(n, 2)).astype(np.float32)).to(ps.device)
+    noise = torch.from_numpy(rng.normal(0, 0.3, size=(n, ps.dim)).astype(np.float32)).to(ps.device)
     ps.v[:n] += torch.where(fl.unsqueeze(1), noise, torch.zeros_like(noise))
     solver.initialize()
     solver.compute_densities()
@@ -50,8 +59,10 @@ def _noalloc(ps, n, offset):
     return out.value
 
 
-def test_noalloc_matches_context_entry_point_twice(cuda):
-    ps, solver = _scene()
+@pytest.mark.parametrize("name", list(SCENES))
+def test_noalloc_matches_context_entry_point_twice(cuda, name):
+    ps, solver = _scene(name)
+    assert bool(ps.params.has_transit) == (name == "channel2d_transit")
     n = ps.particle_num[None]
     solver.compute_density_change()
     ref0 = solver.compute_density_error(0.0)
@@ -66,6 +77,14 @@ def test_noalloc_matches_context_entry_point_twice(cuda):
     for _ in range(2):
         got0 = _noalloc(ps, n, 0.0)
         assert abs(got0 - ref0) <= RTOL * abs(ref0)
+
+
+def test_noalloc_empty_range_is_zero(cuda):
+    ps, solver = _scene()
+    solver.compute_density_change()
+    assert _noalloc(ps, ps.particle_num[None], 0.0) != 0.0  # leaves non-zero partials behind
+    for _ in range(2):
+        assert _noalloc(ps, 0, 0.0) == 0.0
 
 
 def test_noalloc_rejects_sizes_beyond_the_limit(cuda):
