@@ -1,7 +1,13 @@
-"""ASCII PLY export with the reference's header and row format
-(karman_vortex.py:122-214), read from the device buffers in one copy."""
+"""Frame export with the reference's formats (karman_vortex.py:38-214).
+
+PLY frames are written asynchronously: the fields are snapshotted on the
+compute stream (a device-to-device copy, so later steps may overwrite them),
+copied into pinned host buffers on a side stream, and formatted and written
+by a worker thread, so the step loop does not wait for the file."""
 from __future__ import annotations
 
+import threading
+from concurrent.futures import Future, ThreadPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -27,49 +33,129 @@ _HEADER = (
 )
 
 
-def particle_types(ps, obj_id: np.ndarray) -> np.ndarray:
+def particle_types(obj_id: np.ndarray, fluid_blocks, emitters, rigid_blocks, rigid_bodies) -> np.ndarray:
     """0 fluid block, 1 fluid emitter, 2 rigid block, 3 rigid body, 4 other
     (karman_vortex.py:159-179; later assignments win)."""
     t = np.full(obj_id.shape[0], 4, dtype=np.uint8)
-    for ids, code in ((ps.obj_id_fluid_blocks, 0), (ps.obj_id_emitters, 1),
-                      (ps.obj_id_rigid_blocks, 2), (ps.object_id_rigid_body, 3)):
+    for ids, code in ((fluid_blocks, 0), (emitters, 1), (rigid_blocks, 2), (rigid_bodies, 3)):
         if ids:
             t[np.isin(obj_id, np.array(sorted(ids), dtype=obj_id.dtype))] = code
     return t
 
 
-def write_ply(solver, cnt: int, ply_path: Path) -> Path | None:
-    ps = solver.ps
-    n = ps.particle_num[None]
-    if n == 0:
-        return None
-    x = solver.x_temp[:n].cpu().numpy()
-    vort = ps.vorticity[:n].cpu().numpy()
-    color = ps.color[:n].cpu().numpy()
-    obj_id = ps.object_id[:n].cpu().numpy()
-    active = ps.is_active[:n].cpu().numpy().astype(bool)
-    x, vort, color, obj_id = x[active], vort[active], color[active], obj_id[active]
+def _object_sets(ps):
+    return (frozenset(ps.obj_id_fluid_blocks), frozenset(ps.obj_id_emitters),
+            frozenset(ps.obj_id_rigid_blocks), frozenset(ps.object_id_rigid_body))
+
+
+def format_ply(x, vorticity, color, obj_id, is_active, object_sets) -> str | None:
+    """The text of karman_vortex.py:136-214: the active particles' rows,
+    `x y z vort_x vort_y vort_z r g b object_id particle_type`, floats as
+    %.7f; None when no particle is active.  2-D positions get z = 0."""
+    active = np.asarray(is_active).astype(bool)
+    x, vort = np.asarray(x)[active], np.asarray(vorticity)[active]
+    color, obj_id = np.asarray(color)[active], np.asarray(obj_id)[active]
     m = x.shape[0]
     if m == 0:
         return None
     if x.shape[1] == 2:
         x = np.concatenate([x, np.zeros((m, 1), dtype=x.dtype)], axis=1)
-    ptype = particle_types(ps, obj_id)
-    ply_path.mkdir(parents=True, exist_ok=True)
-    path = ply_path / f"frame_{cnt:04}.ply"
+    ptype = particle_types(obj_id, *object_sets)
     cols = [x[:, 0], x[:, 1], x[:, 2], vort[:, 0], vort[:, 1], vort[:, 2]]
-    with open(path, "w") as f:
-        f.write(_HEADER.format(n=m))
-        rows = np.empty(m, dtype=object)
-        fl = [np.char.mod("%.7f", c.astype(np.float64)) for c in cols]
-        ints = [np.char.mod("%d", c) for c in (color[:, 0], color[:, 1], color[:, 2], obj_id, ptype)]
-        parts = fl + ints
-        line = parts[0]
-        for p in parts[1:]:
-            line = np.char.add(np.char.add(line, " "), p)
-        f.write("\n".join(line.tolist()))
-        f.write("\n")
-    return path
+    parts = [np.char.mod("%.7f", c.astype(np.float64)) for c in cols]
+    parts += [np.char.mod("%d", c) for c in (color[:, 0], color[:, 1], color[:, 2], obj_id, ptype)]
+    line = parts[0]
+    for p in parts[1:]:
+        line = np.char.add(np.char.add(line, " "), p)
+    return _HEADER.format(n=m) + "\n".join(line.tolist()) + "\n"
+
+
+class AsyncPlyWriter:
+    """PLY frames of one particle system, written off the step loop.
+
+    `submit` records the frame and returns at once; `flush` waits for every
+    frame and raises the first error.  Two buffer sets are kept, so a third
+    frame in flight waits for the oldest one to be written."""
+
+    FIELDS = ("x_temp", "vorticity", "color", "object_id", "is_active")
+
+    def __init__(self, ps, slots: int = 2):
+        import torch
+        self.ps = ps
+        self.side = torch.cuda.Stream(ps.device)
+        self.pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="ply")
+        self.slots = [None] * slots
+        self.next = 0
+        self.futures: list[Future] = []
+        self.lock = threading.Lock()
+
+    def _sources(self, solver):
+        ps = self.ps
+        return {"x_temp": solver.x_temp, "vorticity": ps.vorticity, "color": ps.color,
+                "object_id": ps.object_id, "is_active": ps.is_active}
+
+    def _slot(self, src, n):
+        import torch
+        k = self.next
+        self.next = (k + 1) % len(self.slots)
+        slot = self.slots[k]
+        if slot is not None and slot["future"] is not None:
+            slot["future"].result()  # the worker is done with these buffers
+        if slot is None or slot["cap"] < n:
+            cap = max(n, 1)
+            slot = {"cap": cap, "future": None, "dev": {}, "pin": {}}
+            for name, t in src.items():
+                shape = (cap,) + tuple(t.shape[1:])
+                slot["dev"][name] = torch.empty(shape, dtype=t.dtype, device=t.device)
+                slot["pin"][name] = torch.empty(shape, dtype=t.dtype, pin_memory=True)
+            self.slots[k] = slot
+        return slot
+
+    def submit(self, solver, cnt: int, ply_path: Path) -> Path | None:
+        import torch
+        ps = self.ps
+        n = ps.particle_num[None]
+        if n == 0:
+            return None
+        src = self._sources(solver)
+        slot = self._slot(src, n)
+        with torch.cuda.stream(ps.stream):
+            for name, t in src.items():
+                slot["dev"][name][:n].copy_(t[:n])
+            snap = torch.cuda.Event()
+            snap.record(ps.stream)
+        self.side.wait_event(snap)
+        with torch.cuda.stream(self.side):
+            for name in src:
+                slot["pin"][name][:n].copy_(slot["dev"][name][:n], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(self.side)
+        ply_path = Path(ply_path)
+        ply_path.mkdir(parents=True, exist_ok=True)
+        path = ply_path / f"frame_{cnt:04}.ply"
+        sets = _object_sets(ps)
+        fut = self.pool.submit(self._write, done, slot, n, sets, path)
+        slot["future"] = fut
+        with self.lock:
+            self.futures.append(fut)
+        return path
+
+    @staticmethod
+    def _write(done, slot, n, sets, path: Path) -> Path | None:
+        done.synchronize()
+        a = {k: v[:n].numpy() for k, v in slot["pin"].items()}
+        text = format_ply(a["x_temp"], a["vorticity"], a["color"], a["object_id"], a["is_active"], sets)
+        if text is None:
+            return None
+        with open(path, "w") as f:
+            f.write(text)
+        return path
+
+    def flush(self):
+        with self.lock:
+            futs, self.futures = self.futures, []
+        for f in futs:
+            f.result()
 
 
 # ------------------------------------------------------------------ PNG

@@ -84,6 +84,14 @@ class KarmanVortexSolver(DIMCVSPHSolver):
 
     def export_ply(self, cnt, ply_path):
         """ASCII PLY with the reference's header and row format
-        (karman_vortex.py:122-214), from device buffers."""
-        from .export import write_ply
-        return write_ply(self, cnt, Path(ply_path))
+        (karman_vortex.py:122-214).  Asynchronous: returns the file's path at
+        once; the file is complete after flush_exports()."""
+        if getattr(self, "_ply_writer", None) is None:
+            from .export import AsyncPlyWriter
+            self._ply_writer = AsyncPlyWriter(self.ps)
+        return self._ply_writer.submit(self, cnt, Path(ply_path))
+
+    def flush_exports(self):
+        """Waits until every PLY frame submitted by export_ply is written."""
+        if getattr(self, "_ply_writer", None) is not None:
+            self._ply_writer.flush()

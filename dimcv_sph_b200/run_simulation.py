@@ -65,6 +65,7 @@ def main(argv=None):
             print(f"wall {time.time() - t0:.1f}s")
         if t > simulation_time or os.path.exists("stop") or (args.max_steps and cnt >= args.max_steps):
             break
+    solver.flush_exports()  # PLY frames are written asynchronously
     return solver
 
 
