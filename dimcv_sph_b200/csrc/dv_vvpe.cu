@@ -630,6 +630,11 @@ __device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+  f2_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 __device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
   f2_t d;
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
@@ -641,21 +646,44 @@ __device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
   return d;
 }
 
+// float4 words per staged sample of the paired loops: the reference kernel
+// needs {x, y, (z,) ω̂z, -ω̂z, (ω̂y, -ω̂x)}, the blob kernel {x, y, z, ω̂, -ω̂}
+template <int D, bool BLOB>
+constexpr int far_x2_words() {
+  return BLOB ? 5 : (D == 3 ? 4 : 2);
+}
+
 // targets [tbase + k·FT2 + tid] (k < TT) of targets[0, nt) against samples
 // [m0, m0 + M); writes far_acc[t] for t < nt.  Block-uniform bounds.
-template <int D, int TT>
+// BLOB (3-D only): the regularised blob kernel, lane for lane the scalar
+// loop's far_accum<3, true, false>: r² by mul + 2 fma, rsqrt(r² + δ²) (one
+// MUFU per lane, scalar), its cube by two multiplies, then six fma into the
+// accumulators; fma(-e, ω̂y, acc) is taken as fma(e, -ω̂y, acc), the same
+// IEEE result.  targets may be null (target t is slot t); n_valid >= 0 zeroes
+// the output of target slots outside [0, n_valid) (the full Biot-Savart's
+// caller-given targets).
+template <int D, int TT, bool BLOB = false>
 __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __restrict__ x,
                                            const int32_t* __restrict__ targets, int nt, int tbase,
                                            const float4* __restrict__ spos, const float4* __restrict__ sw, int m0,
-                                           int M, float4* __restrict__ far_acc, float4* s4) {
+                                           int M, float4* __restrict__ far_acc, float4* s4, int n_valid = -1) {
+  static_assert(!BLOB || D == 3, "the paired blob loop is 3-D");
   constexpr int NP = TT / 2;
-  constexpr int NQ = D == 3 ? 4 : 2;  // duplicated float4 per sample
+  constexpr int NQ = far_x2_words<D, BLOB>();  // duplicated float4 per sample
   f2_t PX[NP], PY[NP], PZ[NP], AX[NP], AY[NP], AZ[NP];
+  bool OK[2 * NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     const int t0 = tbase + (2 * p) * FT2 + threadIdx.x, t1 = tbase + (2 * p + 1) * FT2 + threadIdx.x;
-    const V3 a = ldv<D>(x, targets[t0 < nt ? t0 : nt - 1]);
-    const V3 b = ldv<D>(x, targets[t1 < nt ? t1 : nt - 1]);
+    int i0 = t0 < nt ? t0 : nt - 1, i1 = t1 < nt ? t1 : nt - 1;
+    if (targets) {
+      i0 = targets[i0];
+      i1 = targets[i1];
+    }
+    OK[2 * p] = n_valid < 0 || (i0 >= 0 && i0 < n_valid);
+    OK[2 * p + 1] = n_valid < 0 || (i1 >= 0 && i1 < n_valid);
+    const V3 a = ldv<D>(x, OK[2 * p] ? i0 : 0);
+    const V3 b = ldv<D>(x, OK[2 * p + 1] ? i1 : 0);
     PX[p] = f2_pack(a.x, b.x);
     PY[p] = f2_pack(a.y, b.y);
     PZ[p] = f2_pack(a.z, b.z);
@@ -669,7 +697,13 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
     for (int q = threadIdx.x; q < m; q += FT2) {
       const float4 sp = spos[m0 + base + q];
       const float4 w = sw[m0 + base + q];
-      if (D == 3) {
+      if (BLOB) {
+        s4[5 * q] = make_float4(sp.x, sp.x, sp.y, sp.y);
+        s4[5 * q + 1] = make_float4(sp.z, sp.z, w.z, w.z);
+        s4[5 * q + 2] = make_float4(-w.y, -w.y, w.x, w.x);
+        s4[5 * q + 3] = make_float4(-w.z, -w.z, w.y, w.y);
+        s4[5 * q + 4] = make_float4(-w.x, -w.x, 0.0f, 0.0f);
+      } else if (D == 3) {
         s4[4 * q] = make_float4(sp.x, sp.x, sp.y, sp.y);
         s4[4 * q + 1] = make_float4(sp.z, sp.z, w.z, w.z);
         s4[4 * q + 2] = make_float4(-w.z, -w.z, w.y, w.y);
@@ -680,6 +714,35 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
       }
     }
     __syncthreads();
+    if (BLOB) {
+      const float d2v = P.blob_delta2;
+      const f2_t D2 = f2_pack(d2v, d2v);
+#pragma unroll kFarQUnroll
+      for (int q = 0; q < m; ++q) {
+        const ulonglong2 v0 = s2[NQ * q], v1 = s2[NQ * q + 1], v2 = s2[NQ * q + 2], v3 = s2[NQ * q + 3];
+        const ulonglong2 v4 = s2[NQ * q + 4];
+        const f2_t SZ = v1.x, WZ = v1.y, NWY = v2.x, WX = v2.y, NWZ = v3.x, WY = v3.y, NWX = v4.x;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const f2_t DX = f2_sub(PX[p], v0.x), DY = f2_sub(PY[p], v0.y), DZ = f2_sub(PZ[p], SZ);
+          f2_t R2 = f2_mul(DX, DX);
+          R2 = f2_fma(DY, DY, R2);
+          R2 = f2_fma(DZ, DZ, R2);
+          float sa, sb;
+          f2_unpack(f2_add(R2, D2), sa, sb);
+          const f2_t INV = f2_pack(rsqrtf(sa), rsqrtf(sb));
+          const f2_t KK = f2_mul(f2_mul(INV, INV), INV);
+          const f2_t A = f2_mul(KK, DX), B = f2_mul(KK, DY), E = f2_mul(KK, DZ);
+          AX[p] = f2_fma(B, WZ, AX[p]);
+          AX[p] = f2_fma(E, NWY, AX[p]);
+          AY[p] = f2_fma(E, WX, AY[p]);
+          AY[p] = f2_fma(A, NWZ, AY[p]);
+          AZ[p] = f2_fma(A, WY, AZ[p]);
+          AZ[p] = f2_fma(B, NWX, AZ[p]);
+        }
+      }
+      continue;
+    }
 #pragma unroll kFarQUnroll
     for (int q = 0; q < m; ++q) {
       const ulonglong2 v0 = s2[NQ * q], v1 = s2[NQ * q + 1];
@@ -724,25 +787,25 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
     f2_unpack(AY[p], y0, y1);
     f2_unpack(AZ[p], z0, z1);
     const int t0 = tbase + (2 * p) * FT2 + threadIdx.x, t1 = tbase + (2 * p + 1) * FT2 + threadIdx.x;
-    if (t0 < nt) far_acc[t0] = make_float4(x0, y0, z0, 0.0f);
-    if (t1 < nt) far_acc[t1] = make_float4(x1, y1, z1, 0.0f);
+    if (t0 < nt) far_acc[t0] = OK[2 * p] ? make_float4(x0, y0, z0, 0.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t1 < nt) far_acc[t1] = OK[2 * p + 1] ? make_float4(x1, y1, z1, 0.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
-template <int D, int TT>
+template <int D, int TT, bool BLOB>
 __global__ void __launch_bounds__(FT2, DV_FAR_MINB(TT)) k_far_main_x2(dv_params P, const float* __restrict__ x,
                                                      const dv_counters* __restrict__ C,
                                                      const int32_t* __restrict__ targets,
                                                      const float4* __restrict__ spos,
                                                      const float4* __restrict__ sw, float4* __restrict__ far_acc,
                                                      int nchunk, int64_t stride) {
-  __shared__ float4 s4[(D == 3 ? 4 : 2) * FTILE2];
+  __shared__ float4 s4[far_x2_words<D, BLOB>() * FTILE2];
   const int nt = C->n_targets;
   const int tbase = blockIdx.x * FT2 * TT;
   if (tbase >= nt) return;  // uniform per CTA
   int m0, M;
   sample_chunk(C->num_samples, nchunk, m0, M);
-  far_x2_run<D, TT>(P, x, targets, nt, tbase, spos, sw, m0, M, far_acc + blockIdx.y * stride, s4);
+  far_x2_run<D, TT, BLOB>(P, x, targets, nt, tbase, spos, sw, m0, M, far_acc + blockIdx.y * stride, s4);
 }
 
 template <int D, int TT>
@@ -778,7 +841,9 @@ static inline int far_tile_run(int tt, bool paired) {
 
 template <int D, bool BLOB, bool COMP, bool PER>
 static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt_req) {
-  constexpr bool paired = !BLOB && !COMP && !PER;  // the reference kernel's plain loop
+  // the plain (uncompensated, non-periodic) loops: the reference kernel, and
+  // the blob kernel in 3-D
+  constexpr bool paired = !COMP && !PER && (!BLOB || D == 3);
   const int tt = far_tile_run(tt_req, paired);
   const int64_t nu = std::min<int64_t>(c->n_upper, c->cap);
   const int nb = (int)std::max<int64_t>(1, (nu + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));
@@ -787,8 +852,8 @@ static void launch_main_tt(dv_ctx* c, const dv_fields* f, int tt_req) {
   k_far_main<D, TTV, BLOB, COMP, PER><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
                                                                    c->sw, c->far_acc, c->far_chunks, c->cap)
 #define L2(TTV)                                                                                              \
-  k_far_main_x2<D, TTV><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, c->sw,        \
-                                                     c->far_acc, c->far_chunks, c->cap)
+  k_far_main_x2<D, TTV, BLOB && D == 3><<<grid, FT2, 0, c->stream>>>(c->p, f->x, c->d_cnt, c->targets, c->spos, \
+                                                                     c->sw, c->far_acc, c->far_chunks, c->cap)
   if (tt == 2)
     L(2);
   else if (tt == 4) {
@@ -1269,12 +1334,73 @@ __global__ void __launch_bounds__(FT2) k_bs_fast(dv_params P, const float* __res
   }
 }
 
+// The same sum with two targets per f32x2 instruction (3-D): the grid is
+// (target tiles) x (source chunks), each CTA writes its chunk's partial sums
+// to acc[chunk * stride + t] and k_bs_chunk_sum adds the chunks in order, so
+// the result does not depend on the schedule.  The chunks give a grid of many
+// waves on a 1M x 1M sum, where whole-range CTAs would leave most of the
+// last wave idle.
+template <int TT>
+__global__ void __launch_bounds__(FT2, DV_FAR_MINB(TT)) k_bs_x2(dv_params P, const float* __restrict__ x,
+                                                               const int32_t* __restrict__ tlist, int nt,
+                                                               const float4* __restrict__ spos,
+                                                               const float4* __restrict__ sw,
+                                                               const int32_t* __restrict__ ns_p,
+                                                               const dv_counters* __restrict__ C, int nchunk,
+                                                               int64_t stride, float4* __restrict__ acc) {
+  __shared__ float4 s4[far_x2_words<3, true>() * FTILE2];
+  const int tbase = blockIdx.x * FT2 * TT;
+  if (tbase >= nt) return;  // uniform per CTA
+  const int ns = *ns_p;
+  const int clen = (ns + nchunk - 1) / nchunk;
+  const int m0 = (int)blockIdx.y * clen;
+  const int M = max(0, min(clen, ns - m0));
+  far_x2_run<3, TT, true>(P, x, tlist, nt, tbase, spos, sw, m0, M, acc + blockIdx.y * stride, s4, C->n);
+}
+
+__global__ void k_bs_chunk_sum(const float4* __restrict__ acc, int nt, int nchunk, int64_t stride, float coef,
+                               float* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  float4 a = acc[t];
+  for (int k = 1; k < nchunk; ++k) {
+    const float4 b = acc[k * stride + t];
+    a.x += b.x;
+    a.y += b.y;
+    a.z += b.z;
+  }
+  reinterpret_cast<float4*>(out)[t] = make_float4(a.x * coef, a.y * coef, a.z * coef, 0.0f);
+}
+
+template <int TTV>
+static int launch_bs_x2(dv_ctx* c, const dv_fields* f, const int32_t* targets, int nt, const int32_t* ns,
+                        float* out) {
+  const int64_t tiles = ((int64_t)nt + (int64_t)FT2 * TTV - 1) / ((int64_t)FT2 * TTV);
+  const int64_t resident = (int64_t)c->num_sms * DV_FAR_MINB(TTV) * 256 / FT2;
+  // enough chunks for about eight waves, within the partial-sum buffer
+  const int nchunk =
+      (int)std::max<int64_t>(1, std::min<int64_t>(DV_MAX_FAR_CHUNKS, (8 * resident + tiles - 1) / tiles));
+  const dim3 grid((unsigned)tiles, nchunk);
+  k_bs_x2<TTV><<<grid, FT2, 0, c->stream>>>(c->p, f->x, targets, nt, c->spos, c->sw, ns, c->d_cnt, nchunk, c->cap,
+                                            c->far_acc);
+  DV_LAUNCHED(c);
+  k_bs_chunk_sum<<<dv_blocks(nt), DV_THREADS, 0, c->stream>>>(c->far_acc, nt, nchunk, c->cap, c->p.blob_coef, out);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
 template <int D>
 static int bs_dispatch(dv_ctx* c, const dv_fields* f, const int32_t* targets, int nt, void* out,
                        int precision) {
   const int nb = dv_blocks(nt, FT);
   const bool blob = c->p.kernel_mode == DV_KERNEL_BLOB3D;
   const int32_t* ns = c->d_flag + 2;
+  if (precision == 32 && blob && !c->p.periodic && !c->p.compensated && D == 3 && c->far_tt > 2) {
+    // the paired loop (a tile of 2 keeps the scalar loop below)
+    if (c->far_tt <= 4) return launch_bs_x2<4>(c, f, targets, nt, ns, (float*)out);
+    if (c->far_tt <= 6) return launch_bs_x2<6>(c, f, targets, nt, ns, (float*)out);
+    return launch_bs_x2<8>(c, f, targets, nt, ns, (float*)out);
+  }
   if (precision == 32 && blob && !c->p.periodic) {
     const int tt = c->far_tt <= 2 ? 2 : (c->far_tt <= 4 ? 4 : 8);
     const int nbf = (int)std::max<int64_t>(1, ((int64_t)nt + (int64_t)FT2 * tt - 1) / ((int64_t)FT2 * tt));

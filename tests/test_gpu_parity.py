@@ -297,6 +297,27 @@ def test_full_bs_matches_fp64_oracle(cuda):
         ref = o.bs_full(om, None, n)
         assert relerr(out64.cpu().numpy()[:, :3], ref[:, :3]) < 1e-12, kernel
         assert relerr(out32.cpu().numpy()[:, :3], ref[:, :3]) < RTOL, kernel
+        if kernel == "blob3d":
+            # FP32 blob sum: tile 2 is the scalar loop, 4 / 6 / 8 the paired
+            # loop over source chunks; caller targets outside [0, n) give 0
+            tl = torch.tensor([0, 7, n + 5, n - 1, -3, 11], dtype=torch.int32, device=ps.device)
+            valid = np.array([True, True, False, True, False, True])
+            for tt in (2, 4, 6, 8):
+                assert ps.lib.dv_set_far_tile(ps.ctx, tt) == 0
+                for tgt, cnt in ((None, n), (tl, tl.numel())):
+                    got = torch.full((cnt, 4), float("nan"), dtype=torch.float32, device=ps.device)
+                    tp = C.c_void_p(tgt.data_ptr()) if tgt is not None else None
+                    rc = ps.lib.dv_bs_full(ps.ctx, C.byref(ps.fields_struct), C.c_void_p(om_d.data_ptr()), tp,
+                                           cnt, C.c_void_p(got.data_ptr()), 32)
+                    assert rc == 0, ps.lib.dv_last_error(ps.ctx)
+                    g = got.cpu().numpy()[:, :3]
+                    if tgt is None:
+                        assert relerr(g, ref[:, :3]) < RTOL, (kernel, tt)
+                    else:
+                        idx = tl.cpu().numpy()[valid]
+                        assert relerr(g[valid], ref[idx, :3]) < RTOL, (kernel, tt)
+                        assert np.all(g[~valid] == 0.0), (kernel, tt)
+            assert ps.lib.dv_set_far_tile(ps.ctx, 4) == 0
 
 
 def test_point_vortex_velocity_is_analytic(cuda):
@@ -357,15 +378,21 @@ def test_substep_matches_oracle(cuda, channel):
         for k in ("x", "v", "density", "density_adv", "dfsph_factor"):
             assert relerr(g[k][fl], r[k][fl]) < RTOL, (step, k, relerr(g[k][fl], r[k][fl]))
         bitexact(g["solver.sample_idx"][:M], r["solver.sample_idx"][:M], "samples")
+        # copy_x_temp / compute_vorticity_vis (dimcv_sph.py:778-801): sweeps of
+        # bit-exact inputs, so bit-exact themselves
+        bitexact(g["solver.x_temp"], r["solver.x_temp"], "x_temp")
+        bitexact(g["solver.vorticity_vis"][fl], r["solver.vorticity_vis"][fl], "vorticity_vis")
+        nontrivial(r["solver.vorticity_vis"][fl], "vorticity_vis")
 
 
-@pytest.mark.parametrize("dim", [2, 3])
-def test_paired_fp32_far_loop_is_bit_identical_to_scalar(cuda, dim):
+@pytest.mark.parametrize("case", ["2d", "3d", "blob3d"])
+def test_paired_fp32_far_loop_is_bit_identical_to_scalar(cuda, case):
     """The far-field main loop with two targets per f32x2 instruction (tiles
-    of 4 and 8 targets per thread) gives the same bits as the scalar loop
+    of 4, 6 and 8 targets per thread) gives the same bits as the scalar loop
     (tile of 2): every lane operation is the same IEEE operation in the same
     order.  2-D: the channel; 3-D: the operator-level ring with the
-    reference (2-D-projected) kernel."""
+    reference (2-D-projected) kernel, and with the regularised blob kernel."""
+    dim = 2 if case == "2d" else 3
     out = {}
     if dim == 2:
         ps, solver = make(scenes.channel2d(trim_cylinder=True))
@@ -389,7 +416,7 @@ def test_paired_fp32_far_loop_is_bit_identical_to_scalar(cuda, dim):
             out[tt] = solver.v_vort.clone()
     else:
         from dimcv_sph_b200.ring_study import RingStudy
-        st = RingStudy(n=16384, subset=256, kernel3d=False)
+        st = RingStudy(n=16384, subset=256, kernel3d=case == "blob3d")
         for tt in (2, 4, 6, 8):
             assert st.ps.lib.dv_set_far_tile(st.ps.ctx, tt) == 0
             st.solver.far_tile = tt
