@@ -19,7 +19,6 @@ import argparse
 import ctypes as C
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -33,11 +32,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-steps/s (DFSPH+MC-VVPE) vs full Biot-Savart on 1 B200 at equal vel. error"
 UNIT = "particle-steps/s"
-# Jacobi iterations per solve in the reference arm's bounded samples: the
-# counts the GPU measures on these workloads (divergence 1, pressure 1)
-REF_JACOBI_ITERS = (1, 1)
-# algorithmic FP32 operations per (target, sample) pair of the far field
+# algorithmic FP32 operations per (target, sample) pair of the far field:
+# the reference kernel in 2-D and 3-D, and the 3-D blob kernel (+3)
 FLOPS_PER_PAIR = {2: 12, 3: 24}
+FLOPS_PER_PAIR_BLOB = 27
 
 
 def parse():
@@ -53,6 +51,12 @@ def parse():
                     help="skip the MC-VVPE vs full Biot-Savart study on the 1M-particle vortex ring")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--scale", type=float, default=1.0, help="particle radius multiplier (1 = benchmark size)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra figures: the sphere with the 3-D blob kernel, the 256-scene batch "
+                         "and the adjoint rollout")
+    ap.add_argument("--far-tile", type=int, default=None,
+                    help="far-field targets per thread (2, 4, 6, 8) instead of the autotuner's choice")
+    ap.add_argument("--far-chunks", type=int, default=None, help="far-field sample chunks (1..8)")
     return ap.parse_args()
 
 
@@ -254,13 +258,104 @@ def stage_times(solver, ps, steps: int) -> dict:
     return {k: v / steps for k, v in acc.items()}
 
 
-def read_traffic():
-    """DRAM bytes per far-field launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "vvpe_far_sphere3d.md"
-    if not p.exists():
+def far_traffic(workload: str, tile: int, chunks: int, n_targets: float):
+    """DRAM bytes (read + write) per far-field launch: from the committed
+    capture record of the same workload, tile and sample-chunk count
+    (profiles/far_field_traffic.json, an ncu capture of the 8x smaller case),
+    scaled by the targets of one launch; None when no record matches."""
+    p = ROOT / "profiles" / "far_field_traffic.json"
+    try:
+        recs = json.loads(p.read_text())["captures"]
+    except (OSError, KeyError, ValueError):
         return None
-    m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) if m else None
+    for r in recs:
+        if r["workload"] == workload and r["far_tile"] == tile and r["far_chunks"] == chunks:
+            return {"bytes_per_launch": r["dram_bytes_per_launch"] * n_targets / r["n_targets"],
+                    "capture": {k: r[k] for k in ("scale", "n_targets", "num_samples", "dram_bytes_per_launch",
+                                                  "command")},
+                    "scaled_by": "targets per launch (target reads and partial writes grow with them; the "
+                                 "samples stay L2-resident)"}
+    return None
+
+
+def vvpe_applied(ps, solver) -> dict:
+    """One step with the VVPE's effect counted: the fluid rows whose velocity
+    the gate |v_vort| < |v| (dimcv_sph.py:717-719) let the VVPE change, and
+    the rows with a finite v_vort."""
+    import torch
+    orig = solver.vort2vel
+    rec = {}
+
+    def tap():
+        n = ps.particle_num[None]
+        before = ps.v[:n].clone()
+        orig()
+        fl = ps.material[:n] == 1
+        changed = ((ps.v[:n] != before).any(1) & fl).sum()
+        finite = (torch.isfinite(solver.v_vort[:n]).all(1) & fl).sum()
+        rec.update(fluid=int(fl.sum()), applied=int(changed), finite=int(finite))
+
+    solver.vort2vel = tap
+    try:
+        solver.step()
+    finally:
+        del solver.vort2vel
+    return {"fraction": rec["applied"] / max(1, rec["fluid"]), "finite_fraction": rec["finite"] / max(1, rec["fluid"]),
+            "fluid_rows": rec["fluid"]}
+
+
+def set_far_shape(args, ps, solver):
+    from dimcv_sph_b200 import _lib
+    if args.far_tile:
+        solver.far_tile = args.far_tile
+        _lib.check(ps.ctx, ps.lib.dv_set_far_tile(ps.ctx, args.far_tile), "dv_set_far_tile")
+    if args.far_chunks:
+        _lib.check(ps.ctx, ps.lib.dv_set_far_chunks(ps.ctx, args.far_chunks), "dv_set_far_chunks")
+
+
+def kernel3d_figure(args, steps: int = 10) -> dict:
+    """The sphere workload with the regularised 3-D blob kernel in place of
+    the reference's 2-D projected one (no 0/0 rows, so every fluid row's far
+    field reaches v through the gate test): particle-steps/s and the far
+    field's FP32 roofline."""
+    import torch
+    from dimcv_sph_b200.particle_system import ParticleSystem
+    cfg, config = workload_config(args.workload, args.scale)
+    cfg.config["Configuration"]["kernel3D"] = True
+    ps = ParticleSystem(cfg)
+    solver = ps.build_solver()
+    solver.initialize()
+    set_far_shape(args, ps, solver)
+    lib, ctx = ps.lib, ps.ctx
+    peak = C.c_double(0)
+    lib.dv_fp32_peak(ctx, C.byref(peak))
+    for _ in range(3):
+        solver.step()
+    torch.cuda.synchronize()
+    cnt0 = ps.counters()
+    lib.dv_profile(ctx, 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        solver.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    far_ms, far_launches, pairs = C.c_double(), C.c_int64(), C.c_double()
+    lib.dv_profile_read(ctx, C.byref(far_ms), C.byref(far_launches), C.byref(pairs))
+    lib.dv_profile(ctx, 0)
+    cnt1 = ps.counters()
+    n_fluid = 0.5 * (cnt0["n_fluid"] + cnt1["n_fluid"])
+    ach = FLOPS_PER_PAIR_BLOB * pairs.value / (far_ms.value * 1e-3) / 1e12 if far_ms.value > 0 else 0.0
+    out = {"workload": config["workload"] + "; kernel3D: blob (1/4π) V (ω×r)/(|r|²+δ²)^{3/2}, δ = r",
+           "value": n_fluid * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+           "far_field": {"achieved": round(ach, 3), "peak": round(peak.value / 1e12, 3), "unit": "TFLOP/s",
+                         "frac": round(ach / (peak.value / 1e12), 4) if peak.value else None,
+                         "flops_per_pair": FLOPS_PER_PAIR_BLOB, "kernel_ms_per_step": far_ms.value / steps,
+                         "far_tile_targets_per_thread": solver.far_tile,
+                         "far_sample_chunks": int(lib.dv_get_far_chunks(ctx))},
+           "vvpe_applied": vvpe_applied(ps, solver)}
+    return out
 
 
 def run_ours(args, rank, world, local):
@@ -274,6 +369,7 @@ def run_ours(args, rank, world, local):
     ps = ParticleSystem(cfg, device=dev)
     solver = ps.build_solver()
     solver.initialize()
+    set_far_shape(args, ps, solver)
     lib, ctx = ps.lib, ps.ctx
     peak = C.c_double(0)
     _lib.check(ctx, lib.dv_fp32_peak(ctx, C.byref(peak)), "dv_fp32_peak")
@@ -308,15 +404,19 @@ def run_ours(args, rank, world, local):
     dim = ps.dim
     achieved = FLOPS_PER_PAIR[dim] * pairs.value / (far_ms.value * 1e-3) / 1e12 if far_ms.value > 0 else 0.0
     peak_tf = peak.value / 1e12
-    traffic = read_traffic()
+    far_chunks = int(ps.lib.dv_get_far_chunks(ps.ctx))
+    tr = far_traffic(args.workload if args.scale == 1.0 else f"{args.workload}@{args.scale:g}", solver.far_tile,
+                     far_chunks, cnt1["n_targets"])
     roofline = {"kernel": "k_far_main (Monte-Carlo Biot-Savart far field)", "bound": "fp32",
                 "achieved": round(achieved, 3), "peak": round(peak_tf, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_tf, 4) if peak_tf else None,
-                "traffic": traffic,
+                "traffic": tr["bytes_per_launch"] if tr else None,
                 "peak_source": "measured in this run: FP32 FMA chain kernel (dv_fp32_peak), an FMA counts 2",
                 "flops_per_pair": FLOPS_PER_PAIR[dim], "pairs_per_step": pairs.value / args.steps,
                 "kernel_ms_per_step": far_ms.value / args.steps,
                 "kernel_share_of_step": far_ms.value / ms_local}
+    if tr:
+        roofline["traffic_source"] = tr
 
     result = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
               "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -327,7 +427,7 @@ def run_ours(args, rank, world, local):
               "clocks": clk, "gpu_launches": int(launches), "roofline": roofline,
               "iterations": {"divergence": cnt1["iters_div"], "pressure": cnt1["iters_p"]},
               "far_tile_targets_per_thread": solver.far_tile,
-              "far_sample_chunks": int(ps.lib.dv_get_far_chunks(ps.ctx))}
+              "far_sample_chunks": far_chunks}
 
     # per-stage device times and HBM fractions (outside the timed region)
     st = stage_times(solver, ps, 3)
@@ -335,15 +435,28 @@ def run_ours(args, rank, world, local):
     cnt2 = ps.counters()
     result["stage_roofline"] = stage_roofline(st, dim, cnt2["n"], cnt2["iters_div"], cnt2["iters_p"])
 
+    # the share of fluid rows whose velocity the VVPE changes (one more step)
+    result["vvpe_applied_fraction"] = vvpe_applied(ps, solver)
     if not args.no_e2e:
         result["e2e"] = e2e(args, ps, solver, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args, ps, solver)
-    if rank == 0 and world == 1 and not args.no_vs_bs:
+    if rank == 0 and world == 1:
         del ps, solver
         torch.cuda.empty_cache()
-        from dimcv_sph_b200 import ring_study
-        result["vs_full_bs"] = ring_study.run(n=1 << 20)
+        if not args.no_extras and args.workload == "sphere3d":
+            result["kernel3d"] = kernel3d_figure(args)
+            torch.cuda.empty_cache()
+        if not args.no_vs_bs:
+            from dimcv_sph_b200 import ring_study
+            result["vs_full_bs"] = ring_study.run(n=1 << 20)
+            torch.cuda.empty_cache()
+        if not args.no_extras:
+            from dimcv_sph_b200 import adjoint_study, batch_study
+            result["batch_c4"] = batch_study.run(lone_rounds=2)
+            torch.cuda.empty_cache()
+            result["adjoint_c3"] = adjoint_study.timing()
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -469,6 +582,25 @@ def oracle_scene(cfg):
     return o
 
 
+def jacobi_counts(o):
+    """Iteration counts of the divergence and pressure solves on the full
+    state (densities, factor, divergence solve, non-pressure forces,
+    prediction, pressure solve; the VVPE's small velocity change before the
+    pressure solve is left out).  Returns (it_div, it_p, seconds)."""
+    t0 = time.perf_counter()
+    o.lib.dvo_set_sample(o.ctx, 0, 0x7FFFFFFF, 0, 0)
+    snap = {k: o.f.a[k].copy() for k in ("v", "density", "dfsph_factor", "density_adv", "acceleration")}
+    o.call("densities")
+    o.call("dfsph_factor")
+    it_div = o.divergence_solve()
+    o.call("nonpressure")
+    o.call("predict_velocity")
+    it_p = o.pressure_solve()
+    for k, a in snap.items():
+        o.f.a[k][...] = a
+    return max(1, it_div), max(1, it_p), time.perf_counter() - t0
+
+
 def run_reference(args, rank, world):
     """The reference's CPU path on the host cores.  Taichi (the reference's
     runtime) is not installable here, so the arm runs the oracle port: each
@@ -489,10 +621,10 @@ def run_reference(args, rank, world):
     fl = np.nonzero(o.f["material"][:n] == 1)[0]
     smp = np.sort(rng.choice(fl, size=M, replace=False)).astype(np.int32)
     o.solver["sample_idx"][:M] = smp
+    it_div, it_p, t_solve = jacobi_counts(o)
     budget = max(1.0, 120.0 / max(1, args.steps + args.warmup))
     lo = n // 3
     probe = min(n - lo, 1024)
-    it_div, it_p = REF_JACOBI_ITERS
     per = timed_sample(o, lo, lo + probe, it_div, it_p, M) / probe
     S = int(min(n - lo, max(probe, budget / max(per, 1e-9))))
     tot_t, tot_p = 0.0, 0
@@ -504,7 +636,8 @@ def run_reference(args, rank, world):
             tot_p += sample_fluid(o, a, a + S)
     value = tot_p / tot_t
     sample = (f"each step: 1 substep on {S} of {n} slots (contiguous Morton range) with {M} samples and "
-              f"{it_div}+{it_p} Jacobi iterations; full grid rebuild {t_sort:.2f}s charged pro rata")
+              f"{it_div}+{it_p} Jacobi iterations (measured by one full-state solve, {t_solve:.1f}s); "
+              f"full grid rebuild {t_sort:.2f}s charged pro rata")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, args.steps), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",

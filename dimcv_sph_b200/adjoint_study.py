@@ -42,6 +42,36 @@ def _cos(a, b):
     return float((a * b).sum() / (a.norm() * b.norm()))
 
 
+def timing(n: int = 65536, steps: int = 32, ckpt: int = 8, mc_fraction: float = 1.0 / 16.0, seed: int = 0,
+           target_seed: int = 7, reps: int = 5) -> dict:
+    """Forward and adjoint device times of the C3 rollout alone (the MC
+    Biot-Savart step, checkpoints every ckpt steps): the forward rollout with
+    the loss, and forward + backward; adjoint = the difference."""
+    cfg, x, w = scenes.periodic2d(n, seed=seed, dt=0.01)
+    box = VortexBox(cfg, x, mc_fraction=mc_fraction)
+    dev = box.device
+    w0 = torch.from_numpy(w).to(dev)
+    _, _, wt = scenes.periodic2d(n, seed=target_seed, dt=0.01)
+    with torch.no_grad():
+        target = box.rollout(torch.from_numpy(wt).to(dev), steps, mode=FULL)
+
+    def fwd():
+        with torch.no_grad():
+            return box.loss(box.rollout(w0, steps, checkpoint_every=ckpt, mode=MC), target)
+
+    def fwd_bwd():
+        wg = w0.clone().requires_grad_(True)
+        box.loss(box.rollout(wg, steps, checkpoint_every=ckpt, mode=MC), target).backward()
+
+    fwd()
+    fwd_bwd()
+    t_f = timed(fwd, reps)
+    t_fb = timed(fwd_bwd, reps)
+    return {"workload": f"periodic2d inverse problem: n={n}, {steps}-step rollout, checkpoints every {ckpt}, "
+                        f"M={box.M}", "forward_ms": t_f, "forward_backward_ms": t_fb, "adjoint_ms": t_fb - t_f,
+            "adjoint_over_forward": (t_fb - t_f) / t_f}
+
+
 def run(n: int = 65536, steps: int = 32, ckpt: int = 8, mc_fraction: float = 1.0 / 16.0,
         Rs=(1, 4, 16, 64), opt_iters: int = 40, lr: float = 0.2, fd_coords: int = 64, seed: int = 0,
         target_seed: int = 7) -> dict:

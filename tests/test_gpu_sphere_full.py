@@ -1,0 +1,142 @@
+"""One step of the benchmark scene itself against the oracle.
+
+The flow past a sphere at r = 0.004 (2.37M slots, about 2M fluid) is the
+workload the bench times.  Its first step (emission, grid build, substep) is
+run stage by stage on the GPU in the order of ``karman_vortex.py:232-242``,
+with the oracle (Morton visit order) loaded with the same state:
+
+* DFSPH fields (density, factor, density_adv, v, acceleration) bit-exact and
+  the Jacobi iteration counts equal;
+* the DIMCV sweeps (vorticity, d_vort_smoothed, KVN, kden) bit-exact, the
+  FP64 kden_sum equal, the M = N_fluid/32 inverse-CDF samples identical;
+* the Monte-Carlo far field on a fixed 65,536-slot range of targets against
+  the oracle's FP64 sum: the same NaN rows (the reference's 2-D projected
+  near field in 3-D), the rest within 1e-5;
+* from the GPU's velocity after the VVPE on, life time, the pressure solve,
+  the vis sweep and advection bit-exact, iteration counts equal.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from dimcv_sph_b200 import scenes
+from oracle.oracle import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+SUBSET = 65536
+
+
+def _g(ps, name, n):
+    if name.startswith("solver."):
+        return ps.solver_buf.t[name[7:]][:n].cpu().numpy()
+    return ps.fields.t[name][:n].cpu().numpy()
+
+
+def _o(o, name, n):
+    if name.startswith("solver."):
+        return o.solver.a[name[7:]][:n]
+    return o.f.a[name][:n]
+
+
+def _bitexact(ps, o, names, n, stage):
+    for k in names:
+        a, b = _g(ps, k, n), _o(o, k, n)
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
+        assert np.all(same), (stage, k, int(np.count_nonzero(~same)))
+
+
+def test_benchmark_scene_step_matches_oracle(cuda):
+    from dimcv_sph_b200.particle_system import ParticleSystem
+    ps = ParticleSystem(scenes.sphere3d())
+    solver = ps.build_solver()
+    solver.track_iterations = True
+    solver.initialize()
+    # KarmanVortexSolver.step (karman_vortex.py:216-230) up to the substep
+    if solver.cnt % solver.emit_interval == 0:
+        solver.emit_particle()
+    solver.cnt += 1
+    ps.initialize_particle_system()
+    c = ps.counters()
+    n, nf = c["n"], c["n_fluid"]
+    assert n > 2_000_000 and nf > 1_900_000
+    o = OracleSim(ps.params, ps.particle_max_num, 0)
+    o.load_snapshot(ps.snapshot(), c)
+    o.counting_sort()
+    assert np.array_equal(o.permutation(), np.arange(n))
+    M = max(1, int(nf / 32))
+    solver.mc_samples = M
+
+    # DFSPH: densities, factor, divergence solve, non-pressure forces
+    solver.compute_densities()
+    solver.compute_DFSPH_factor()
+    solver.divergence_solve()
+    solver.compute_non_pressure_forces()
+    o.call("densities")
+    o.call("dfsph_factor")
+    it_div = o.divergence_solve()
+    o.call("nonpressure")
+    assert solver.last_iters[0] == it_div
+    _bitexact(ps, o, ["density", "dfsph_factor", "density_adv", "v", "acceleration"], n, "dfsph")
+
+    # DIMCV sweeps and the inverse-CDF samples
+    solver.init()
+    solver.compute_d_vorticity()
+    solver.compute_all_d_vort_smoothed()
+    solver.update_sample()
+    solver.compute_kernel_density()
+    solver._draw_samples()
+    o.calls("dimcv_vorticity")
+    o.calls("d_vorticity")
+    o.calls("smooth_d_vort")
+    o.calls("kvn_sample", solver.seed, solver.rng_step, 0)
+    o.calls("akde")
+    o.calls("sample", 1, solver.seed, solver.rng_step, M)
+    _bitexact(ps, o, ["vorticity", "solver.d_vort_smoothed", "solver.kvn", "solver.kden"], n, "dimcv")
+    assert ps.counters()["kden_sum"] == o.counters()["kden_sum"]
+    assert ps.counters()["num_samples"] == M
+    assert np.array_equal(_g(ps, "solver.sample_idx", M), _o(o, "solver.sample_idx", M))
+
+    # VVPE: all targets on the GPU, a fixed slot range in FP64 on the oracle
+    v_before = _g(ps, "v", n).copy()
+    solver.vort2vel()
+    lo = n // 3
+    hi = lo + SUBSET
+    o.lib.dvo_set_sample(o.ctx, lo, hi, 0, 0)
+    o.calls("vvpe_mc", 64)
+    o.lib.dvo_set_sample(o.ctx, 0, 0x7FFFFFFF, 0, 0)
+    mat = _g(ps, "material", n)
+    fl = mat[lo:hi] == 1
+    gv = _g(ps, "solver.v_vort", n)[lo:hi][fl][:, :3]
+    rv = _o(o, "solver.v_vort", n)[lo:hi][fl][:, :3]
+    assert fl.sum() > 30000
+    assert np.array_equal(np.isnan(gv), np.isnan(rv))
+    fin = np.isfinite(rv).all(axis=1)
+    assert fin.sum() > 0
+    err = float(np.max(np.abs(gv[fin].astype(np.float64) - rv[fin])) / np.max(np.abs(rv[fin])))
+    assert err < RTOL, err
+    v_after = _g(ps, "v", n)
+    flall = mat == 1
+    applied = np.any(v_after != v_before, axis=1) & flall
+    # continue both from the GPU's post-VVPE velocity
+    o.f.a["v"][:n] = v_after
+
+    # life time, velocity prediction, pressure solve, vis, advection
+    solver.update_particle_life_time()
+    solver.predict_velocity()
+    solver.pressure_solve()
+    solver.copy_x_temp()
+    solver.advect()
+    o.call("life_time")
+    o.call("predict_velocity")
+    it_p = o.pressure_solve()
+    o.calls("vis")
+    o.call("advect")
+    assert solver.last_iters[1] == it_p
+    _bitexact(ps, o, ["life_time", "v", "density_adv", "x", "solver.x_temp", "solver.vorticity_vis"], n,
+              "pressure+advect")
+    print(json.dumps({"n": n, "n_fluid": nf, "M": M, "iterations": [it_div, it_p], "vvpe_rel_err": err,
+                      "subset_fluid": int(fl.sum()), "subset_finite_rows": int(fin.sum()),
+                      "vvpe_applied_fraction": float(applied.sum() / flall.sum())}))
