@@ -223,6 +223,16 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// 1/sqrt(x) in one MUFU operation.  The blob kernel's argument |r|² + δ² is
+// at least δ² > 0 and never subnormal, so flushing subnormals changes no
+// result; without .ftz the approximate rsqrt also carries the code that
+// rescales subnormal inputs, which every pair would pay for.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // coordinate difference, minimum image on a periodic box
 template <bool PER>
 __device__ __forceinline__ float wrapd(float d, float L) {
@@ -248,7 +258,7 @@ __device__ __forceinline__ void far_terms(float px, float py, float pz, float4 s
     cy = -__fmul_rn(a, w.z);
     cz = __fmaf_rn(a, w.y, -__fmul_rn(b, w.x));
   } else {
-    const float inv = rsqrtf(__fadd_rn(r2, d2));
+    const float inv = rsqrt_approx(__fadd_rn(r2, d2));
     const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
     cx = __fmaf_rn(b, w.z, -__fmul_rn(e, w.y));
@@ -284,7 +294,7 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
       az.s = __fmaf_rn(-b, w.x, az.s);
     }
   } else {
-    const float inv = rsqrtf(__fadd_rn(r2, d2));
+    const float inv = rsqrt_approx(__fadd_rn(r2, d2));
     const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
     ax.s = __fmaf_rn(b, w.z, ax.s);
@@ -730,7 +740,7 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
           R2 = f2_fma(DZ, DZ, R2);
           float sa, sb;
           f2_unpack(f2_add(R2, D2), sa, sb);
-          const f2_t INV = f2_pack(rsqrtf(sa), rsqrtf(sb));
+          const f2_t INV = f2_pack(rsqrt_approx(sa), rsqrt_approx(sb));
           const f2_t KK = f2_mul(f2_mul(INV, INV), INV);
           const f2_t A = f2_mul(KK, DX), B = f2_mul(KK, DY), E = f2_mul(KK, DZ);
           AX[p] = f2_fma(B, WZ, AX[p]);

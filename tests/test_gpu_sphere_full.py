@@ -8,7 +8,8 @@ with the oracle (Morton visit order) loaded with the same state:
 * DFSPH fields (density, factor, density_adv, v, acceleration) bit-exact and
   the Jacobi iteration counts equal;
 * the DIMCV sweeps (vorticity, d_vort_smoothed, KVN, kden) bit-exact, the
-  FP64 kden_sum equal, the M = N_fluid/32 inverse-CDF samples identical;
+  FP64 kden_sum equal to FP64 rounding (1e-12; a block tree on the GPU, slot
+  order on the oracle), the M = N_fluid/32 inverse-CDF samples identical;
 * the Monte-Carlo far field on a fixed 65,536-slot range of targets against
   the oracle's FP64 sum: the same NaN rows (the reference's 2-D projected
   near field in 3-D), the rest within 1e-5;
@@ -95,7 +96,10 @@ def test_benchmark_scene_step_matches_oracle(cuda):
     o.calls("akde")
     o.calls("sample", 1, solver.seed, solver.rng_step, M)
     _bitexact(ps, o, ["vorticity", "solver.d_vort_smoothed", "solver.kvn", "solver.kden"], n, "dimcv")
-    assert ps.counters()["kden_sum"] == o.counters()["kden_sum"]
+    # FP64 sums of the same f32 terms, in a block tree on the GPU and in slot
+    # order on the oracle: equal to FP64 rounding
+    ks, ko = ps.counters()["kden_sum"], o.counters()["kden_sum"]
+    assert abs(ks - ko) <= 1e-12 * abs(ko), (ks, ko)
     assert ps.counters()["num_samples"] == M
     assert np.array_equal(_g(ps, "solver.sample_idx", M), _o(o, "solver.sample_idx", M))
 
