@@ -181,7 +181,7 @@ STAGES = {
     "dfsph": ["compute_densities", "compute_DFSPH_factor", "divergence_solve", "compute_non_pressure_forces",
               "predict_velocity", "pressure_solve"],
     "dimcv_sweeps": ["init", "compute_d_vorticity", "compute_all_d_vort_smoothed", "update_sample",
-                     "compute_kernel_density", "_draw_samples"],
+                     "compute_kernel_density", "smooth_and_kernel_density", "_draw_samples"],
     "vvpe": ["vort2vel"],
     "integrate_vis": ["update_particle_life_time", "copy_x_temp", "advect"],
 }

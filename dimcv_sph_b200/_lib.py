@@ -40,6 +40,7 @@ PROTOTYPES = {
     "dv_boundary_volume": (C.c_int, [_P, _FP]),
     "dv_densities": (C.c_int, [_P, _FP]),
     "dv_dfsph_factor": (C.c_int, [_P, _FP]),
+    "dv_densities_factor": (C.c_int, [_P, _FP]),
     "dv_scale_factor": (C.c_int, [_P, _FP, f32]),
     "dv_density_change": (C.c_int, [_P, _FP]),
     "dv_density_adv": (C.c_int, [_P, _FP]),
@@ -56,6 +57,8 @@ PROTOTYPES = {
     "dv_enforce_boundary": (C.c_int, [_P, _FP, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dv_dimcv_vorticity": (C.c_int, [_P, _FP, _SP]),
     "dv_d_vorticity": (C.c_int, [_P, _FP, _SP]),
+    "dv_vorticity_dvort": (C.c_int, [_P, _FP, _SP]),
+    "dv_smooth_akde": (C.c_int, [_P, _FP, _SP]),
     "dv_smooth_d_vort": (C.c_int, [_P, _FP, _SP]),
     "dv_kvn_sample": (C.c_int, [_P, _FP, _SP, u64, u64, i32]),
     "dv_record_samples": (C.c_int, [_P, _FP, _SP]),

@@ -466,18 +466,17 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
     k_batch_counts<3><<<S, 1024, 0, c->stream>>>(c->p, *dst, b->d_state);
   DV_LAUNCHED(c);
   // substep (karman_vortex.py:232-242)
-  DV_TRY(dv_densities(c, dst));
-  DV_TRY(dv_dfsph_factor(c, dst));
+  DV_TRY(dv_densities_factor(c, dst));  // compute_densities + compute_DFSPH_factor, one sweep
   DV_TRY(dv_density_change(c, dst));
   DV_TRY(dv_scale_factor(c, dst, c->p.inv_dt));
   DV_TRY(dv_batch_solve(c, dst, 0));
   DV_TRY(dv_scale_factor(c, dst, c->p.dt));
   DV_TRY(dv_nonpressure(c, dst));
-  DV_TRY(dv_dimcv_vorticity(c, dst, s));
-  DV_TRY(dv_d_vorticity(c, dst, s));
-  DV_TRY(dv_smooth_d_vort(c, dst, s));
+  // v*, ω, ∇v and Δω in one sweep; KVN (independent of the smoothing) before
+  // the sweep that smooths Δω and sums the AKDE
+  DV_TRY(dv_vorticity_dvort(c, dst, s));
   DV_TRY(dv_kvn_sample(c, dst, s, 0, 0, 0));
-  DV_TRY(dv_akde(c, dst, s));
+  DV_TRY(dv_smooth_akde(c, dst, s));
   if (c->p.dim == 2)
     k_batch_kden<2><<<S, 1024, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
   else

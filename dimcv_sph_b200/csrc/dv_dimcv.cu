@@ -84,6 +84,60 @@ __global__ void k_d_vorticity(dv_params P, DevGrid G, dv_fields F, dv_solver_fie
   st4(S.d_vort, i, V3{w.x - curl.x, w.y - curl.y, w.z - curl.z});
 }
 
+// k_vorticity and k_d_vorticity in one neighbour walk: v*_j = v_j + a_j·dt
+// is formed per neighbour by the same multiply and add that k_vorticity
+// stores v*_j with, so every sum (ω, ∇v, ∇×v*) and Δω are bit-identical to
+// the two separate sweeps, without re-reading the list, positions and
+// materials or storing and gathering v*.
+template <int D>
+__global__ void k_vorticity_dvort(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                                  const dv_counters* __restrict__ C) {
+  FOR_I;
+  const int DD = D * D;
+  if (F.material[i] != DV_MATERIAL_FLUID) {
+    stv<D>(S.v_star, i, V3{0.f, 0.f, 0.f});
+    st4(F.vorticity, i, V3{0.f, 0.f, 0.f});
+    for (int k = 0; k < DD; ++k) S.grad_v[(int64_t)i * DD + k] = 0.0f;
+    st4(S.d_vort, i, V3{0.f, 0.f, 0.f});
+    return;
+  }
+  V3 xi = ldv<D>(F.x, i);
+  V3 vi = ldv<D>(F.v, i);
+  V3 ai = ldv<D>(F.acceleration, i);
+  V3 vs{vi.x + ai.x * P.dt, vi.y + ai.y * P.dt, D == 3 ? vi.z + ai.z * P.dt : 0.0f};
+  stv<D>(S.v_star, i, vs);
+  V3 w{0.f, 0.f, 0.f};
+  V3 curl{0.f, 0.f, 0.f};
+  float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj != DV_MATERIAL_FLUID) return;
+    V3 vj = ldv<D>(F.v, j);
+    V3 aj = ldv<D>(F.acceleration, j);
+    V3 vsj{vj.x + aj.x * P.dt, vj.y + aj.y * P.dt, D == 3 ? vj.z + aj.z * P.dt : 0.0f};
+    V3 gw = cubic_gradW<D>(P, r, r2);
+    float mv = F.m_V[j];
+    V3 c = cross3(sub3(vj, vi), gw);
+    w.x += mv * c.x;
+    w.y += mv * c.y;
+    w.z += mv * c.z;
+    V3 vji = sub3(vj, vi);
+    float vc[3] = {vji.x, vji.y, vji.z};
+    float gc[3] = {gw.x, gw.y, gw.z};
+#pragma unroll
+    for (int a = 0; a < D; ++a)
+#pragma unroll
+      for (int b = 0; b < D; ++b) g[a * D + b] += (mv * vc[a]) * gc[b];
+    V3 c2 = cross3(sub3(vsj, vs), gw);
+    curl.x += mv * c2.x;
+    curl.y += mv * c2.y;
+    curl.z += mv * c2.z;
+  });
+  st4(F.vorticity, i, w);
+#pragma unroll
+  for (int k = 0; k < DD; ++k) S.grad_v[(int64_t)i * DD + k] = g[k];
+  st4(S.d_vort, i, V3{w.x - curl.x, w.y - curl.y, w.z - curl.z});
+}
+
 // compute_all_d_vort_smoothed (dimcv_sph.py:660-677); slots outside the
 // vortex domain keep their previous value (index-stable field)
 template <int D>
@@ -237,6 +291,43 @@ __global__ void k_akde(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
       for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float, int mj) {
         if (mj == DV_MATERIAL_FLUID) kd += S.kvn[j] * epan<D>(P, r);
       });
+      S.kden[i] = kd;
+      contrib = (double)kd;
+    }
+  }
+  double s = block_sum<double>(contrib);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// k_smooth and k_akde in one neighbour walk (both over the fluid neighbours
+// of a vortex-domain fluid slot): the smoothed Δω and kden of slot i and
+// the FP64 block partials of kden_sum come out bit-identical to the two
+// separate sweeps.  KVN must be current (k_kvn_sample first); the smoothing
+// does not read it.
+template <int D>
+__global__ void k_smooth_akde(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                              const dv_counters* __restrict__ C, double* __restrict__ part) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double contrib = 0.0;
+  if (i < C->n && F.material[i] == DV_MATERIAL_FLUID) {
+    V3 xi = ldv<D>(F.x, i);
+    if (in_vortex_domain<D>(P, xi)) {
+      float mvi = F.m_V[i];
+      V3 di = ld4(S.d_vort, i);
+      float w0 = cubic_W(P, 0.0f);
+      V3 acc{mvi * di.x * w0, mvi * di.y * w0, mvi * di.z * w0};
+      float kd = S.kvn[i] * epan<D>(P, V3{0.f, 0.f, 0.f});
+      for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+        if (mj != DV_MATERIAL_FLUID) return;
+        float mv = F.m_V[j];
+        V3 dj = ld4(S.d_vort, j);
+        float wk = cubic_W(P, sqrtf(r2));
+        acc.x += mv * dj.x * wk;
+        acc.y += mv * dj.y * wk;
+        acc.z += mv * dj.z * wk;
+        kd += S.kvn[j] * epan<D>(P, r);
+      });
+      st4(S.d_vort_smoothed, i, acc);
       S.kden[i] = kd;
       contrib = (double)kd;
     }
@@ -480,6 +571,13 @@ DV_API int dv_dimcv_vorticity(dv_ctx* c, const dv_fields* f, const dv_solver_fie
   return DV_OK;
 }
 
+DV_API int dv_vorticity_dvort(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
+  if (!c || !f) return DV_EINVAL;
+  if (int rc = check_solver(c, s)) return rc;
+  LAUNCH_D(k_vorticity_dvort, nblk(c), c->p, dv_grid(c), *f, *s, c->d_cnt);
+  return DV_OK;
+}
+
 DV_API int dv_d_vorticity(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   if (!c || !f) return DV_EINVAL;
   if (int rc = check_solver(c, s)) return rc;
@@ -524,6 +622,16 @@ DV_API int dv_akde(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
   if (int rc = check_solver(c, s)) return rc;
   const int nb = nblk(c);
   LAUNCH_D(k_akde, nb, c->p, dv_grid(c), *f, *s, c->d_cnt, c->red_part);
+  k_akde_finalize<<<1, 1024, 0, c->stream>>>(c->red_part, nb, c->d_cnt);
+  DV_LAUNCHED(c);
+  return DV_OK;
+}
+
+DV_API int dv_smooth_akde(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s) {
+  if (!c || !f) return DV_EINVAL;
+  if (int rc = check_solver(c, s)) return rc;
+  const int nb = nblk(c);
+  LAUNCH_D(k_smooth_akde, nb, c->p, dv_grid(c), *f, *s, c->d_cnt, c->red_part);
   k_akde_finalize<<<1, 1024, 0, c->stream>>>(c->red_part, nb, c->d_cnt);
   DV_LAUNCHED(c);
   return DV_OK;

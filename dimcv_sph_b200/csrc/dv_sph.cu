@@ -76,6 +76,48 @@ __global__ void k_dfsph_factor(dv_params P, DevGrid G, dv_fields F, const dv_cou
   F.dfsph_factor[i] = sum_k > P.factor_min ? 1.0f / sum_k : 0.0f;
 }
 
+// compute_densities + compute_DFSPH_factor in one neighbour walk: the two
+// reference sweeps visit the same neighbours in the same order, and each sum
+// here is built by the same operations in that order, so density and factor
+// are bit-identical to k_densities and k_dfsph_factor; the list, position and
+// material of each neighbour are read once instead of twice.
+template <int D>
+__global__ void k_densities_factor(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  FOR_I;
+  if (F.material[i] != DV_MATERIAL_FLUID) return;
+  V3 xi = ldv<D>(F.x, i);
+  float dens = F.m_V[i] * cubic_W(P, 0.0f);
+  float den = 0.0f;
+  V3 gi{0.f, 0.f, 0.f};
+  float sum_k = 0.0f;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj == DV_MATERIAL_FLUID) {
+      const float mvj = F.m_V[j];
+      den += mvj * cubic_W(P, sqrtf(r2));
+      V3 gw = cubic_gradW<D>(P, r, r2);
+      float mm = F.m[j];
+      V3 g{mm * gw.x, mm * gw.y, mm * gw.z};
+      sum_k += sqnorm<D>(g);
+      gi.x += g.x;
+      gi.y += g.y;
+      if (D == 3) gi.z += g.z;
+    } else if (mj == DV_MATERIAL_SOLID) {
+      const float mvj = F.m_V[j];
+      den += mvj * cubic_W(P, sqrtf(r2));
+      V3 gw = cubic_gradW<D>(P, r, r2);
+      float s = mvj * P.density0;
+      gi.x += s * gw.x;
+      gi.y += s * gw.y;
+      if (D == 3) gi.z += s * gw.z;
+    }
+  });
+  dens += den;
+  dens *= P.density0;
+  F.density[i] = dens;
+  sum_k += sqnorm<D>(gi);
+  F.dfsph_factor[i] = sum_k > P.factor_min ? 1.0f / sum_k : 0.0f;
+}
+
 // multiply_time_step (dimcv_sph.py:395-399)
 __global__ void k_scale_factor(dv_fields F, float s, const dv_counters* __restrict__ C) {
   FOR_I;
@@ -527,6 +569,12 @@ DV_API int dv_densities(dv_ctx* c, const dv_fields* f) {
 DV_API int dv_dfsph_factor(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
   LAUNCH_D(k_dfsph_factor, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_densities_factor(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_densities_factor, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
   return DV_OK;
 }
 

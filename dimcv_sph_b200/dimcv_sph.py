@@ -150,11 +150,26 @@ class DIMCVSPHSolver(SPHBase):
         self._calls("dv_sample", DV_SAMPLE_INJECTED, 0, 0, int(value))
 
     # ----------------------------------------------------------- DFSPH
+    # Sweeps that the reference runs back to back over the same neighbours
+    # are fused (dv_densities_factor, dv_vorticity_dvort): the first method
+    # computes both results and the second skips its sweep when no library
+    # kernel has run since, so nothing it reads can have changed through the
+    # library (a caller that edits the fields with torch in between calls the
+    # library entry point of the second sweep itself).
+    _fused_factor_at = -1
+    _fused_dvort_at = -1
+
+    def _launches(self):
+        return self.lib.dv_launch_count(self.ctx)
+
     def compute_DFSPH_factor(self):  # dimcv_sph.py:86-106
+        if self._fused_factor_at == self._launches():
+            return  # computed by compute_densities' sweep, bit-identical
         self._call("dv_dfsph_factor")
 
-    def compute_densities(self):  # :139-148
-        self._call("dv_densities")
+    def compute_densities(self):  # :139-148 (with :86-106 in the same sweep)
+        self._call("dv_densities_factor")
+        self._fused_factor_at = self._launches()
 
     def compute_non_pressure_forces(self):  # :195-208
         self._call("dv_nonpressure")
@@ -222,10 +237,13 @@ class DIMCVSPHSolver(SPHBase):
     def compute_grad_v(self):  # :273-282
         self._calls("dv_dimcv_vorticity")
 
-    def init(self):  # :803-806 — one fused sweep for v*, ω and ∇v
-        self._calls("dv_dimcv_vorticity")
+    def init(self):  # :803-806 — one sweep for v*, ω and ∇v, and Δω (:573-583) with them
+        self._calls("dv_vorticity_dvort")
+        self._fused_dvort_at = self._launches()
 
     def compute_d_vorticity(self):  # :573-583
+        if self._fused_dvort_at == self._launches():
+            return  # computed by init's sweep, bit-identical
         self._calls("dv_d_vorticity")
 
     def compute_all_d_vort_smoothed(self):  # :666-677
@@ -285,12 +303,19 @@ class DIMCVSPHSolver(SPHBase):
     def compute_vorticity_vis(self):  # :785-795 — done by copy_x_temp's fused sweep
         pass
 
+    def smooth_and_kernel_density(self):
+        """compute_all_d_vort_smoothed + compute_kernel_density (:660-677,
+        738-751) in one sweep; needs this step's KVN (update_sample first)."""
+        self._calls("dv_smooth_akde")
+
     def dimcv(self):  # :812-819
         self.init()
         self.compute_d_vorticity()
-        self.compute_all_d_vort_smoothed()
+        # KVN and the birth/death draws read only ∇v, life time and the sample
+        # flags, and the smoothing reads none of what they write, so they run
+        # first and the smoothing shares the AKDE's neighbour sweep
         self.update_sample()
-        self.compute_kernel_density()
+        self.smooth_and_kernel_density()
         self._draw_samples()
         self.vort2vel()
         self.update_particle_life_time()

@@ -275,6 +275,10 @@ DV_API int dv_set_dynamic_rigid(dv_ctx* ctx, int32_t on);
 DV_API int dv_densities(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.compute_DFSPH_factor (dimcv_sph.py:86-124). */
 DV_API int dv_dfsph_factor(dv_ctx* ctx, const dv_fields* f);
+/* compute_densities followed by compute_DFSPH_factor (dimcv_sph.py:86-148)
+ * in one neighbour sweep: both fields bit-identical to dv_densities then
+ * dv_dfsph_factor. */
+DV_API int dv_densities_factor(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.multiply_time_step(dfsph_factor, s) (dimcv_sph.py:395-399). */
 DV_API int dv_scale_factor(dv_ctx* ctx, const dv_fields* f, float s);
 /* DIMCVSPHSolver.compute_density_change (dimcv_sph.py:337-374). */
@@ -316,6 +320,10 @@ DV_API int dv_enforce_boundary(dv_ctx* ctx, const dv_fields* f, int32_t material
 DV_API int dv_dimcv_vorticity(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
 /* compute_d_vorticity (dimcv_sph.py:551-583). */
 DV_API int dv_d_vorticity(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
+/* dv_dimcv_vorticity followed by dv_d_vorticity (dimcv_sph.py:228-293,
+ * 551-583) in one neighbour sweep, v*_j formed per neighbour: v_star,
+ * vorticity, grad_v and d_vort bit-identical to the two calls. */
+DV_API int dv_vorticity_dvort(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
 /* compute_all_d_vort_smoothed (dimcv_sph.py:660-677). */
 DV_API int dv_smooth_d_vort(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
 /* compute_kinematic_vorticity_num_sample (dimcv_sph.py:295-324): KVN and
@@ -329,6 +337,11 @@ DV_API int dv_kvn_sample(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields
 DV_API int dv_record_samples(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
 /* compute_kernel_density (dimcv_sph.py:721-751); kden_sum is reduced in FP64. */
 DV_API int dv_akde(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
+/* compute_all_d_vort_smoothed and compute_kernel_density (dimcv_sph.py:
+ * 660-677, 721-751) in one neighbour sweep: d_vort_smoothed, kden and
+ * kden_sum bit-identical to dv_smooth_d_vort then dv_akde.  Needs the KVN of
+ * this step (dv_kvn_sample first; the smoothing does not depend on it). */
+DV_API int dv_smooth_akde(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s);
 /* New (no reference counterpart): FP64 CDF of kden over the VVPE targets
  * and M i.i.d. inverse-CDF draws (Philox keyed by seed, step, draw) into
  * sample_idx; or, for DV_SAMPLE_INJECTED, adopt num_samples = M with

@@ -441,3 +441,56 @@ def test_paired_fp32_far_loop_is_bit_identical_to_scalar(cuda, case):
     ok = np.isfinite(r)
     assert np.array_equal(np.isfinite(g), ok)
     assert relerr(g[ok], r[ok]) < 1e-5
+
+
+@pytest.mark.parametrize("scene", ["channel2d", "sphere3d_coarse"])
+def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
+    """dv_densities_factor, dv_vorticity_dvort and dv_smooth_akde give the
+    same bits as the pairs of sweeps they replace."""
+    cfg = scenes.channel2d(trim_cylinder=True) if scene == "channel2d" else scenes.sphere3d(radius=0.016)
+    ps, solver = make(cfg)
+    solver.initialize()
+    solver._call("dv_nonpressure")
+
+    def snap(names):
+        g = ps.snapshot()
+        return {k: g[k].copy() for k in names}
+
+    solver._call("dv_densities")
+    solver._call("dv_dfsph_factor")
+    a = snap(["density", "dfsph_factor"])
+    ps.density.zero_()
+    ps.dfsph_factor.zero_()
+    solver._call("dv_densities_factor")
+    b = snap(["density", "dfsph_factor"])
+    for k in a:
+        bitexact(b[k], a[k], k)
+    nontrivial(a["dfsph_factor"], "factor")
+
+    names = ["solver.v_star", "vorticity", "solver.grad_v", "solver.d_vort"]
+    solver._calls("dv_dimcv_vorticity")
+    solver._calls("dv_d_vorticity")
+    a = snap(names)
+    for k in ("v_star", "grad_v", "d_vort"):
+        ps.solver_buf.t[k].zero_()
+    ps.fields.t["vorticity"].zero_()
+    solver._calls("dv_vorticity_dvort")
+    b = snap(names)
+    for k in names:
+        bitexact(b[k], a[k], k)
+    nontrivial(a["solver.d_vort"], "d_vort")
+
+    solver._calls("dv_kvn_sample", 0, 0, 0)
+    solver._calls("dv_smooth_d_vort")
+    solver._calls("dv_akde")
+    names = ["solver.d_vort_smoothed", "solver.kden"]
+    a = snap(names)
+    ka = ps.counters()["kden_sum"]
+    ps.solver_buf.t["d_vort_smoothed"].zero_()
+    ps.solver_buf.t["kden"].zero_()
+    solver._calls("dv_smooth_akde")
+    b = snap(names)
+    for k in names:
+        bitexact(b[k], a[k], k)
+    assert ps.counters()["kden_sum"] == ka
+    nontrivial(a["solver.kden"], "kden")
