@@ -233,6 +233,19 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return r;
 }
 
+// The blob kernel's (|r|² + δ²)^(-3/2): s = δ² + dx² + dy² + dz² by three
+// fma (δ² enters first, saving an add), then 1/s · 1/sqrt(s) from two MUFU
+// operations and one multiply instead of the cube of 1/sqrt(s) (two
+// multiplies): 16 FP32-pipe operations per pair instead of 18 in a loop the
+// FP32 pipe bounds, one more on the otherwise idle MUFU.  The scalar loop,
+// the paired loop and the near-sample correction all use this one form.
+__device__ __forceinline__ float blob_k(float dx, float dy, float dz, float d2) {
+  float s = __fmaf_rn(dx, dx, d2);
+  s = __fmaf_rn(dy, dy, s);
+  s = __fmaf_rn(dz, dz, s);
+  return __fmul_rn(rcp_approx(s), rsqrt_approx(s));
+}
+
 // coordinate difference, minimum image on a periodic box
 template <bool PER>
 __device__ __forceinline__ float wrapd(float d, float L) {
@@ -247,10 +260,10 @@ __device__ __forceinline__ void far_terms(float px, float py, float pz, float4 s
   const float dx = wrapd<PER>(__fsub_rn(px, sp.x), bx.x);
   const float dy = wrapd<PER>(__fsub_rn(py, sp.y), bx.y);
   const float dz = D == 3 ? wrapd<PER>(__fsub_rn(pz, sp.z), bx.z) : 0.0f;
-  float r2 = __fmul_rn(dx, dx);
-  r2 = __fmaf_rn(dy, dy, r2);
-  if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
   if (!BLOB) {
+    float r2 = __fmul_rn(dx, dx);
+    r2 = __fmaf_rn(dy, dy, r2);
+    if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
     // Kε = 1/|r|² (exp term underflows for |r| > h); cross with r_xy = (dx, dy, 0)
     const float kk = rcp_approx(fmaxf(r2, lim));
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy);
@@ -258,8 +271,7 @@ __device__ __forceinline__ void far_terms(float px, float py, float pz, float4 s
     cy = -__fmul_rn(a, w.z);
     cz = __fmaf_rn(a, w.y, -__fmul_rn(b, w.x));
   } else {
-    const float inv = rsqrt_approx(__fadd_rn(r2, d2));
-    const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
+    const float kk = blob_k(dx, dy, dz, d2);
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
     cx = __fmaf_rn(b, w.z, -__fmul_rn(e, w.y));
     cy = __fmaf_rn(e, w.x, -__fmul_rn(a, w.z));
@@ -275,9 +287,6 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
   const float dx = wrapd<PER>(__fsub_rn(px, sp.x), bx.x);
   const float dy = wrapd<PER>(__fsub_rn(py, sp.y), bx.y);
   const float dz = D == 3 ? wrapd<PER>(__fsub_rn(pz, sp.z), bx.z) : 0.0f;
-  float r2 = __fmul_rn(dx, dx);
-  r2 = __fmaf_rn(dy, dy, r2);
-  if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
   if (COMP) {
     float cx, cy, cz;
     far_terms<D, BLOB, PER>(px, py, pz, sp, w, lim, d2, cx, cy, cz, bx);
@@ -285,6 +294,9 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
     ay.add(cy);
     az.add(cz);
   } else if (!BLOB) {
+    float r2 = __fmul_rn(dx, dx);
+    r2 = __fmaf_rn(dy, dy, r2);
+    if (D == 3) r2 = __fmaf_rn(dz, dz, r2);
     const float kk = rcp_approx(fmaxf(r2, lim));
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy);
     ax.s = __fmaf_rn(b, w.z, ax.s);
@@ -294,8 +306,7 @@ __device__ __forceinline__ void far_accum(float px, float py, float pz, float4 s
       az.s = __fmaf_rn(-b, w.x, az.s);
     }
   } else {
-    const float inv = rsqrt_approx(__fadd_rn(r2, d2));
-    const float kk = __fmul_rn(__fmul_rn(inv, inv), inv);
+    const float kk = blob_k(dx, dy, dz, d2);
     const float a = __fmul_rn(kk, dx), b = __fmul_rn(kk, dy), e = __fmul_rn(kk, dz);
     ax.s = __fmaf_rn(b, w.z, ax.s);
     ax.s = __fmaf_rn(-e, w.y, ax.s);
@@ -640,11 +651,6 @@ __device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
-__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
-  f2_t d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 __device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
   f2_t d;
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
@@ -666,8 +672,8 @@ constexpr int far_x2_words() {
 // targets [tbase + k·FT2 + tid] (k < TT) of targets[0, nt) against samples
 // [m0, m0 + M); writes far_acc[t] for t < nt.  Block-uniform bounds.
 // BLOB (3-D only): the regularised blob kernel, lane for lane the scalar
-// loop's far_accum<3, true, false>: r² by mul + 2 fma, rsqrt(r² + δ²) (one
-// MUFU per lane, scalar), its cube by two multiplies, then six fma into the
+// loop's far_accum<3, true, false>: blob_k's three fma and its two MUFU
+// operations per lane (scalar) and one multiply, then six fma into the
 // accumulators; fma(-e, ω̂y, acc) is taken as fma(e, -ω̂y, acc), the same
 // IEEE result.  targets may be null (target t is slot t); n_valid >= 0 zeroes
 // the output of target slots outside [0, n_valid) (the full Biot-Savart's
@@ -735,13 +741,12 @@ __device__ __forceinline__ void far_x2_run(const dv_params& P, const float* __re
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
           const f2_t DX = f2_sub(PX[p], v0.x), DY = f2_sub(PY[p], v0.y), DZ = f2_sub(PZ[p], SZ);
-          f2_t R2 = f2_mul(DX, DX);
-          R2 = f2_fma(DY, DY, R2);
-          R2 = f2_fma(DZ, DZ, R2);
+          f2_t S2 = f2_fma(DX, DX, D2);
+          S2 = f2_fma(DY, DY, S2);
+          S2 = f2_fma(DZ, DZ, S2);
           float sa, sb;
-          f2_unpack(f2_add(R2, D2), sa, sb);
-          const f2_t INV = f2_pack(rsqrt_approx(sa), rsqrt_approx(sb));
-          const f2_t KK = f2_mul(f2_mul(INV, INV), INV);
+          f2_unpack(S2, sa, sb);
+          const f2_t KK = f2_mul(f2_pack(rcp_approx(sa), rcp_approx(sb)), f2_pack(rsqrt_approx(sa), rsqrt_approx(sb)));
           const f2_t A = f2_mul(KK, DX), B = f2_mul(KK, DY), E = f2_mul(KK, DZ);
           AX[p] = f2_fma(B, WZ, AX[p]);
           AX[p] = f2_fma(E, NWY, AX[p]);

@@ -1,9 +1,10 @@
 """One step of the benchmark scene itself against the oracle.
 
 The flow past a sphere at r = 0.004 (2.37M slots, about 2M fluid) is the
-workload the bench times.  Its first step (emission, grid build, substep) is
-run stage by stage on the GPU in the order of ``karman_vortex.py:232-242``,
-with the oracle (Morton visit order) loaded with the same state:
+workload the bench times.  After 30 steps, its next step (grid build,
+substep) is run stage by stage on the GPU in the order of
+``karman_vortex.py:232-242``, with the oracle (Morton visit order) loaded
+with the same state:
 
 * DFSPH fields (density, factor, density_adv, v, acceleration) bit-exact and
   the Jacobi iteration counts equal;
@@ -28,6 +29,7 @@ pytestmark = pytest.mark.gpu
 
 RTOL = 1e-5
 SUBSET = 65536
+WARM_STEPS = 30
 
 
 def _g(ps, name, n):
@@ -55,6 +57,11 @@ def test_benchmark_scene_step_matches_oracle(cuda):
     solver = ps.build_solver()
     solver.track_iterations = True
     solver.initialize()
+    # 30 steps first: on the emitted lattice every fluid particle has a
+    # neighbour straight above it, so the reference's 2-D projected near field
+    # is 0/0 on every row until the solves' rounding moves particles off it
+    for _ in range(WARM_STEPS):
+        solver.step()
     # KarmanVortexSolver.step (karman_vortex.py:216-230) up to the substep
     if solver.cnt % solver.emit_interval == 0:
         solver.emit_particle()
