@@ -205,7 +205,7 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   c->nbr_cap = cap * (params->dim == 3 ? 48 : 24);
   A(c->nbr_off, cap + 1);
   A(c->nbr_idx, c->nbr_cap);
-  A(c->d_nbr_ok, 1);
+  A(c->d_nbr_ok, 2);  // [0]: lists valid, [1]: a material other than fluid / solid seen by the build
   // the 3-D build's first pass stores up to 64 neighbours per particle in
   // fixed rows (a settled lattice has at most 36); 2-D builds have none
   c->nbr_slots = params->dim == 3 ? 64 : 0;
@@ -217,7 +217,7 @@ DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream
   if (e == cudaSuccess) e = cudaMemset(c->d_cnt, 0, sizeof(dv_counters));
   if (e == cudaSuccess) e = cudaMemset(c->d_flag, 0, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(c->d_prof, 0, sizeof(double) * 4);
-  if (e == cudaSuccess) e = cudaMemset(c->d_nbr_ok, 0, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemset(c->d_nbr_ok, 0, 2 * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMemset(c->cell_start, 0, sizeof(int32_t) * c->ncells);
   if (e == cudaSuccess) e = cudaMemset(c->cell_end, 0, sizeof(int32_t) * c->ncells);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();

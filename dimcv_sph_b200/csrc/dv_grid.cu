@@ -272,12 +272,21 @@ __global__ void k_finalize_counts(const int32_t* __restrict__ part, int nparts,
 // the same order, so the cell scan (3^d cells) is done once here and the
 // sweeps read the lists as CSR (offsets = exclusive scan of the counts).
 //
+// Each entry carries the neighbour's material in its top bit (DV_NBR_SOLID),
+// so the sweeps do not gather it; a material other than fluid or solid sets
+// bad[0] and the lists are not used.
+//
 // 3-D (27 cells, ~8 candidates each): one cell-scan pass stores each
 // particle's first `slots` neighbours in its own fixed row and its count; a
 // warp-wide copy then moves the rows into CSR (a particle with more
 // neighbours than slots scans its cells again there).  This saves a second
 // 27-cell scan.  2-D (9 cells): counting is cheap and the fixed rows cost
 // more write traffic than they save, so a count pass and a fill pass.
+__device__ __forceinline__ int32_t nbr_entry(int j, int mj, int32_t* bad) {
+  if (mj != DV_MATERIAL_FLUID && mj != DV_MATERIAL_SOLID) *bad = 1;
+  return (int32_t)((uint32_t)j | (mj == DV_MATERIAL_SOLID ? DV_NBR_SOLID : 0u));
+}
+
 template <int D>
 __global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
                             const dv_counters* __restrict__ C, int m, uint32_t* __restrict__ cnt) {
@@ -290,25 +299,27 @@ __global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
 
 template <int D>
 __global__ void k_csr_fill(dv_params P, DevGrid G, const float* __restrict__ x,
-                           const dv_counters* __restrict__ C, const uint32_t* __restrict__ off,
-                           const int32_t* __restrict__ ok, int32_t* __restrict__ out) {
+                           const int32_t* __restrict__ mat, const dv_counters* __restrict__ C,
+                           const uint32_t* __restrict__ off, int32_t* __restrict__ ok,
+                           int32_t* __restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C->n || !*ok) return;
+  if (i >= C->n || !ok[0]) return;
   uint32_t k = off[i];
-  for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) { out[k++] = j; });
+  for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i),
+                         [&](int j, V3, float, int mj) { out[k++] = nbr_entry(j, mj, ok + 1); });
 }
 
 template <int D>
-__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x,
+__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
                            const dv_counters* __restrict__ C, int m, int slots, uint32_t* __restrict__ cnt,
-                           int32_t* __restrict__ rows) {
+                           int32_t* __restrict__ rows, int32_t* __restrict__ bad) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   uint32_t k = 0;
   if (i < C->n) {
     int32_t* row = rows + (int64_t)i * slots;
-    for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) {
-      if (k < (uint32_t)slots) row[k] = j;
+    for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i), [&](int j, V3, float, int mj) {
+      if (k < (uint32_t)slots) row[k] = nbr_entry(j, mj, bad);
       ++k;
     });
   }
@@ -318,11 +329,11 @@ __global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x,
 // one warp per group of 32 particles; each row is copied by the whole warp
 // (coalesced reads of the row, coalesced writes of the CSR segment)
 template <int D>
-__global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ x,
+__global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
                               const dv_counters* __restrict__ C, int slots, const int32_t* __restrict__ rows,
-                              const uint32_t* __restrict__ off, const int32_t* __restrict__ ok,
+                              const uint32_t* __restrict__ off, int32_t* __restrict__ ok,
                               int32_t* __restrict__ out) {
-  if (!*ok) return;
+  if (!ok[0]) return;
   const int n = C->n;
   const int lane = threadIdx.x & 31;
   const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31;
@@ -334,14 +345,21 @@ __global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ 
       for (uint32_t k = lane; k < cnt; k += 32) out[k0 + k] = row[k];
     } else if (lane == (i & 31)) {
       uint32_t k = k0;
-      for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) { out[k++] = j; });
+      for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i),
+                             [&](int j, V3, float, int mj) { out[k++] = nbr_entry(j, mj, ok + 1); });
     }
   }
 }
 
 __global__ void k_csr_ok(const uint32_t* __restrict__ off, const dv_counters* __restrict__ C, int64_t cap,
                          int32_t* __restrict__ ok) {
-  *ok = (int64_t)off[C->n] <= cap ? 1 : 0;
+  ok[0] = (int64_t)off[C->n] <= cap ? 1 : 0;
+}
+
+// after the fill: lists that met a material other than fluid or solid are
+// not used (their entries cannot encode it)
+__global__ void k_csr_material_check(int32_t* __restrict__ ok) {
+  if (ok[1]) ok[0] = 0;
 }
 
 static int build_csr(dv_ctx* c, const dv_fields* f) {
@@ -349,9 +367,10 @@ static int build_csr(dv_ctx* c, const dv_fields* f) {
   const int nb = dv_blocks(m);
   DevGrid G = dv_grid_cells(c);
   const bool rows = c->p.dim == 3;
+  DV_CK(c, cudaMemsetAsync(c->d_nbr_ok + 1, 0, sizeof(int32_t), c->stream));
   if (rows)
-    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->nbr_slots, c->flags,
-                                                    c->nbr_rows);
+    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, c->d_cnt, m, c->nbr_slots,
+                                                    c->flags, c->nbr_rows, c->d_nbr_ok + 1);
   else
     k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
   DV_LAUNCHED(c);
@@ -360,11 +379,13 @@ static int build_csr(dv_ctx* c, const dv_fields* f) {
   k_csr_ok<<<1, 1, 0, c->stream>>>(c->nbr_off, c->d_cnt, c->nbr_cap, c->d_nbr_ok);
   DV_LAUNCHED(c);
   if (rows)
-    k_csr_compact<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_slots, c->nbr_rows,
-                                                       c->nbr_off, c->d_nbr_ok, c->nbr_idx);
+    k_csr_compact<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, c->d_cnt, c->nbr_slots,
+                                                       c->nbr_rows, c->nbr_off, c->d_nbr_ok, c->nbr_idx);
   else
-    k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, c->nbr_off, c->d_nbr_ok,
-                                                    c->nbr_idx);
+    k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, c->d_cnt, c->nbr_off,
+                                                    c->d_nbr_ok, c->nbr_idx);
+  DV_LAUNCHED(c);
+  k_csr_material_check<<<1, 1, 0, c->stream>>>(c->d_nbr_ok);
   DV_LAUNCHED(c);
   return DV_OK;
 }
@@ -552,6 +573,11 @@ __global__ void k_u32_to_i64(const uint32_t* __restrict__ a, int64_t* __restrict
   if (i < m) b[i] = a[i];
 }
 
+__global__ void k_nbr_slots(const int32_t* __restrict__ in, int64_t m, int32_t* __restrict__ out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) out[k] = nbr_slot((uint32_t)in[k]);
+}
+
 DV_API int64_t dv_stored_lists(dv_ctx* c, uint32_t* dev_offsets, int32_t* dev_nbrs, int64_t max_entries) {
   if (!c) return DV_EINVAL;
   dv_counters cnt;
@@ -572,9 +598,10 @@ DV_API int64_t dv_stored_lists(dv_ctx* c, uint32_t* dev_offsets, int32_t* dev_nb
     if (total > max_entries)
       return dv_fail(c, DV_ECAPACITY, "dv_stored_lists: %lld entries > max_entries %lld", (long long)total,
                      (long long)max_entries);
-    if (total > 0)
-      DV_CK(c, cudaMemcpyAsync(dev_nbrs, c->nbr_idx, sizeof(int32_t) * (size_t)total, cudaMemcpyDeviceToDevice,
-                               c->stream));
+    if (total > 0) {  // the slots, without the material bit
+      k_nbr_slots<<<dv_blocks(total), DV_THREADS, 0, c->stream>>>(c->nbr_idx, total, dev_nbrs);
+      DV_LAUNCHED(c);
+    }
   }
   DV_CK(c, cudaStreamSynchronize(c->stream));
   return total;

@@ -77,7 +77,7 @@ struct dv_ctx {
   uint32_t* nbr_off = nullptr;  // cap + 1
   int32_t* nbr_idx = nullptr;   // nbr_cap
   int64_t nbr_cap = 0;
-  int32_t* d_nbr_ok = nullptr;  // 1 while the lists match the current positions
+  int32_t* d_nbr_ok = nullptr;  // [0]: 1 while the lists match the current positions; [1]: build scratch
   int32_t* nbr_rows = nullptr;  // 3-D: cap * nbr_slots, the first pass's fixed row of particle i at i * nbr_slots
   int nbr_slots = 0;
 
@@ -349,8 +349,17 @@ __device__ __forceinline__ float transit_weight(const dv_params& P, float x0) {
 // tested exactly as r2 < nbr_r2_limit (sqrtf is monotone, so
 // sqrtf(r2) < h  <=>  r2 < the smallest float whose sqrtf reaches h).
 // f(j, r, r2) receives r = x_i - x_j; for_each_neighbor_m also passes the
-// neighbour's material mj = mat[j], loaded with its index and position one
-// neighbour ahead on the list path (f need not gather it itself).
+// neighbour's material mj (fluid or solid): on the list path it is the top
+// bit of the list entry (DV_NBR_SOLID), so it costs no load; on the
+// cell-scan path it is mat[j].
+// A stored list entry: the neighbour's slot in the low 31 bits, bit 31 set
+// for a solid neighbour.  The list build marks the lists invalid when it
+// meets a material other than fluid or solid, so the sweeps then scan cells.
+#define DV_NBR_SOLID 0x80000000u
+#define DV_NBR_SLOT 0x7fffffffu
+__device__ __forceinline__ int nbr_slot(uint32_t e) { return (int)(e & DV_NBR_SLOT); }
+__device__ __forceinline__ int nbr_mat(uint32_t e) { return (e & DV_NBR_SOLID) ? DV_MATERIAL_SOLID : DV_MATERIAL_FLUID; }
+
 template <int D, bool MAT, typename F>
 __device__ __forceinline__ void for_each_neighbor_impl(const dv_params& P, const DevGrid& G,
                                                        const float* __restrict__ x,
@@ -359,19 +368,21 @@ __device__ __forceinline__ void for_each_neighbor_impl(const dv_params& P, const
     uint32_t k = __ldg(G.noff + i);
     const uint32_t k1 = __ldg(G.noff + i + 1);
     if (k >= k1) return;
-    // one-deep software pipeline: the next neighbour's index and position
-    // (and material) are loaded before f runs on the current one (f still
-    // runs in list order).  Sweeps -5% at 2.37M particles; a two-deep
-    // pipeline was slower.
-    int j = __ldg(G.nidx + k);
+    // one-deep software pipeline: the next neighbour's entry and position
+    // are loaded before f runs on the current one (f still runs in list
+    // order).  Sweeps -5% at 2.37M particles; a two-deep pipeline was slower.
+    const uint32_t* __restrict__ nl = reinterpret_cast<const uint32_t*>(G.nidx);
+    uint32_t e = __ldg(nl + k);
+    int j = nbr_slot(e);
     V3 xj = ldv<D>(x, j);
-    int mj = MAT ? __ldg(mat + j) : 0;
+    int mj = nbr_mat(e);
 #pragma unroll 1
     while (true) {
       const bool more = ++k < k1;
-      const int jn = more ? __ldg(G.nidx + k) : j;
+      const uint32_t en = more ? __ldg(nl + k) : e;
+      const int jn = nbr_slot(en);
       const V3 xn = ldv<D>(x, jn);
-      const int mn = MAT ? __ldg(mat + jn) : 0;
+      const int mn = nbr_mat(en);
       V3 r = rel<D>(P, xi, xj);
       if constexpr (MAT)
         f(j, r, sqnorm<D>(r), mj);

@@ -642,7 +642,7 @@ __global__ void k_plan_slots(dv_params P, DevGrid G, dv_fields F, dv_solver_fiel
   float Si = S.kden[i];
   int near = mult[i];
   for (uint32_t k = k0; k < k1; ++k) {
-    const int j = G.nidx[k];
+    const int j = nbr_slot((uint32_t)G.nidx[k]);
     p.nbr[k] = j;
     if (F.material[j] == DV_MATERIAL_FLUID) Si += S.kden[j];
     near += mult[j];
