@@ -91,7 +91,7 @@ class RingStudy:
         return e0.elapsed_time(e1) / reps
 
 
-def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=3, subset=262144, reps=3, target_err=0.02,
+def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=8, subset=262144, reps=3, target_err=0.02,
         device="cuda") -> dict:
     st = RingStudy(n=n, subset=subset, device=device)
     out = {"n": n, "subset": int(st.sub.numel()), "kernel": "blob3d (1/4π) V (r×ω)/(|r|²+δ²)^{3/2}, δ = r",
@@ -103,9 +103,21 @@ def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=3
         err = float(torch.sqrt(((u32 - st.uref) ** 2).sum(1).mean())) / st.uref_rms
         out["bs_f32_vs_f64"]["compensated" if comp else "plain"] = err
     st.set_compensated(False)
-    bs_ms = st.timed(st.bs_step, 1)
+    # the full-BS step at its best far tile (the paired loop's 4, 6 or 8
+    # targets per thread); the MC steps below autotune their own
+    lib, ctx = st.ps.lib, st.ps.ctx
+    tiles = {}
+    for tt in (4, 6, 8):
+        _lib.check(ctx, lib.dv_set_far_tile(ctx, tt), "dv_set_far_tile")
+        tiles[tt] = st.timed(st.bs_step, 1)
+    best = min(tiles, key=tiles.get)
+    _lib.check(ctx, lib.dv_set_far_tile(ctx, best), "dv_set_far_tile")
+    bs_ms = st.timed(st.bs_step, 2)
     out["bs_step_ms"] = bs_ms
+    out["bs_far_tile"] = best
+    out["bs_tile_sweep_ms"] = {str(k): v for k, v in tiles.items()}
     out["bs_particle_steps_per_s"] = n / (bs_ms * 1e-3)
+    out["bs_tflops_incl_grid"] = 27.0 * n * (n - 1) / (bs_ms * 1e-3) / 1e12
     for mode_name, mode in (("iid", DV_SAMPLE_INVERSE_CDF), ("stratified", DV_SAMPLE_STRATIFIED)):
         for M in Ms:
             errs = []
