@@ -13,7 +13,8 @@ Reports (one JSON object):
     plans and periodic images frozen;
   * FP32 adjoint vs FP64 adjoint on the same frozen plans;
   * MC adjoint vs the full Biot-Savart adjoint: one gradient and the mean of
-    R independent sampler streams (unbiasedness: error ~ R^-1/2);
+    R independent sampler streams (unbiasedness: error ~ R^-1/2), and one
+    stream with M from N/16 to N samples per step (error and cost);
   * Adam on the initial vorticity with MC gradients and with full-BS
     gradients, the loss measured with the full Biot-Savart forward.
 """
@@ -164,6 +165,18 @@ def run(n: int = 65536, steps: int = 32, ckpt: int = 8, mc_fraction: float = 1.0
         m = acc / R
         sweep.append({"R": R, "rel_err": _nrel(m.cpu(), gref.cpu()), "cos": _cos(m.cpu(), gref.cpu())})
     out["mc_vs_full_grad"] = sweep
+
+    # the other way to cut the variance: more samples in each step's plan
+    # (one sampler stream, M from N/16 to N), with the cost of a gradient
+    M0 = box.M
+    msweep = []
+    for frac in (1.0 / 16.0, 0.25, 0.5, 1.0):
+        box.M = max(1, int(round(frac * n)))
+        g1 = grad(MC, 3000)
+        msweep.append({"M": box.M, "rel_err": _nrel(g1.cpu(), gref.cpu()), "cos": _cos(g1.cpu(), gref.cpu()),
+                       "forward_backward_ms": timed(fwd_bwd, 3)})
+    box.M = M0
+    out["mc_grad_vs_M"] = msweep
 
     # ---------------------------------------------------------- inversion
     def true_loss(wv):
