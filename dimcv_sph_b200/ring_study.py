@@ -64,7 +64,7 @@ class RingStudy:
         ps, s = self.ps, self.solver
         ps.v[: self.n] = self.v0
         ps.initialize_particle_system()
-        s.init()
+        s._calls("dv_dimcv_vorticity")  # ∇v for KVN (the step's Δω is not used here)
         s.compute_kinematic_vorticity_num_sample()
         s.compute_kernel_density()
         s._calls("dv_sample", mode, s.seed, seed_step, int(M))

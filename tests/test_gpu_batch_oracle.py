@@ -90,11 +90,21 @@ def _compare(b, s, st, o, M, it, tag):
     return worst
 
 
+def _initial_states(b):
+    """Scene ranges of the batch as built (the device states are set by the
+    first step): scenes in order, each with its initial counts."""
+    st, o = [], 0
+    for n, nf, ns in b.snap_counts:
+        st.append({"start": o, "end": o + n, "n_fluid": nf, "n_solid": ns})
+        o += n
+    return st
+
+
 def test_scene_batch_matches_oracle_every_step(cfgs):
     from dimcv_sph_b200.batch import SceneBatch
-    b = SceneBatch(cfgs)
+    b = SceneBatch(cfgs, keep_snapshots=True)
     params = [_scene_params(c, b.grid_num) for c in cfgs]
-    st = b.states()
+    st = _initial_states(b)
     for step in range(34):
         oracles = [_load_scene(b, s, st, *params[s]) for s in range(b.S)]
         b.step()
@@ -108,10 +118,10 @@ def test_scene_batch_matches_oracle_every_step(cfgs):
 
 def test_one_scene_graph_matches_oracle(cfgs):
     from dimcv_sph_b200.batch import SceneBatch
-    b = SceneBatch(cfgs[1:2])
+    b = SceneBatch(cfgs[1:2], keep_snapshots=True)
     params = _scene_params(cfgs[1], b.grid_num)
     b.capture(2)
-    st = b.states()
+    st = _initial_states(b)
     step = 0
     for _ in range(15):
         o = _load_scene(b, 0, st, *params)
