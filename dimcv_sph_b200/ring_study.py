@@ -139,3 +139,30 @@ def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=8
         ok = [m for m in out["mc"] if m["sampler"] == mode_name and m["rms_err_mean"] <= target_err]
         out["matched"][mode_name] = min(ok, key=lambda m: m["M"]) if ok else None
     return out
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="MC-VVPE vs full Biot-Savart on the 3-D vortex ring")
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--seeds", type=int, default=8)
+    ap.add_argument("--bs-only", action="store_true",
+                    help="only build the ring and run the FP32 full Biot-Savart sum --reps times (a small case "
+                         "for a profiler capture of the paired blob loop)")
+    ap.add_argument("--tile", type=int, default=6, help="targets per thread of the paired loop (--bs-only)")
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+    if a.bs_only:
+        st = RingStudy(n=a.n, subset=min(1024, a.n))
+        _lib.check(st.ps.ctx, st.ps.lib.dv_set_far_tile(st.ps.ctx, a.tile), "dv_set_far_tile")
+        for _ in range(a.reps):
+            st.bs(None, st.n, 32)
+        torch.cuda.synchronize()
+        print(json.dumps({"n": a.n, "tile": a.tile, "bs_ms": st.timed(lambda: st.bs(None, st.n, 32), a.reps)}))
+        return
+    print(json.dumps(run(n=a.n, seeds=a.seeds)))
+
+
+if __name__ == "__main__":
+    main()
