@@ -310,16 +310,16 @@ __global__ void k_csr_fill(dv_params P, DevGrid G, const float* __restrict__ x,
 }
 
 template <int D>
-__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
+__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x,
                            const dv_counters* __restrict__ C, int m, int slots, uint32_t* __restrict__ cnt,
-                           int32_t* __restrict__ rows, int32_t* __restrict__ bad) {
+                           int32_t* __restrict__ rows) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   uint32_t k = 0;
   if (i < C->n) {
     int32_t* row = rows + (int64_t)i * slots;
-    for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i), [&](int j, V3, float, int mj) {
-      if (k < (uint32_t)slots) row[k] = nbr_entry(j, mj, bad);
+    for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) {
+      if (k < (uint32_t)slots) row[k] = j;
       ++k;
     });
   }
@@ -327,7 +327,9 @@ __global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x, 
 }
 
 // one warp per group of 32 particles; each row is copied by the whole warp
-// (coalesced reads of the row, coalesced writes of the CSR segment)
+// (coalesced reads of the row, coalesced writes of the CSR segment), and the
+// neighbours' materials are gathered here, 32 independent loads at a time,
+// rather than in the row scan's dependent chain
 template <int D>
 __global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
                               const dv_counters* __restrict__ C, int slots, const int32_t* __restrict__ rows,
@@ -342,7 +344,10 @@ __global__ void k_csr_compact(dv_params P, DevGrid G, const float* __restrict__ 
     const uint32_t k0 = off[i], cnt = off[i + 1] - k0;
     if (cnt <= (uint32_t)slots) {
       const int32_t* row = rows + (int64_t)i * slots;
-      for (uint32_t k = lane; k < cnt; k += 32) out[k0 + k] = row[k];
+      for (uint32_t k = lane; k < cnt; k += 32) {
+        const int j = row[k];
+        out[k0 + k] = nbr_entry(j, __ldg(mat + j), ok + 1);
+      }
     } else if (lane == (i & 31)) {
       uint32_t k = k0;
       for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i),
@@ -369,8 +374,8 @@ static int build_csr(dv_ctx* c, const dv_fields* f) {
   const bool rows = c->p.dim == 3;
   DV_CK(c, cudaMemsetAsync(c->d_nbr_ok + 1, 0, sizeof(int32_t), c->stream));
   if (rows)
-    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, c->d_cnt, m, c->nbr_slots,
-                                                    c->flags, c->nbr_rows, c->d_nbr_ok + 1);
+    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->nbr_slots, c->flags,
+                                                    c->nbr_rows);
   else
     k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
   DV_LAUNCHED(c);

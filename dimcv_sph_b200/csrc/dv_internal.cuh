@@ -423,15 +423,11 @@ __device__ __forceinline__ void for_each_neighbor_impl(const dv_params& P, const
 #pragma unroll 1
         for (int j = s; j < e; ++j) {
           if (j == i) continue;
-          // the material is loaded with the position, not after the
-          // distance test: the two loads overlap (the cell's slots are
-          // contiguous, so the extra ones hit L1)
-          const int mj = MAT ? __ldg(mat + j) : 0;
           V3 r = rel<D>(P, xi, ldv<D>(x, j));
           float r2 = sqnorm<D>(r);
           if (r2 < lim) {
             if constexpr (MAT)
-              f(j, r, r2, mj);
+              f(j, r, r2, __ldg(mat + j));
             else
               f(j, r, r2);
           }
