@@ -41,6 +41,7 @@ PROTOTYPES = {
     "dv_densities": (C.c_int, [_P, _FP]),
     "dv_dfsph_factor": (C.c_int, [_P, _FP]),
     "dv_densities_factor": (C.c_int, [_P, _FP]),
+    "dv_densities_factor_change": (C.c_int, [_P, _FP]),
     "dv_scale_factor": (C.c_int, [_P, _FP, f32]),
     "dv_density_change": (C.c_int, [_P, _FP]),
     "dv_density_adv": (C.c_int, [_P, _FP]),
@@ -48,6 +49,7 @@ PROTOTYPES = {
     "dv_divergence_iteration": (C.c_int, [_P, _FP]),
     "dv_pressure_iteration": (C.c_int, [_P, _FP]),
     "dv_divergence_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
+    "dv_divergence_solve_prepared": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_pressure_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_nonpressure": (C.c_int, [_P, _FP]),
     "dv_predict_velocity": (C.c_int, [_P, _FP]),

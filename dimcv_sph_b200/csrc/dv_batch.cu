@@ -466,8 +466,9 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
     k_batch_counts<3><<<S, 1024, 0, c->stream>>>(c->p, *dst, b->d_state);
   DV_LAUNCHED(c);
   // substep (karman_vortex.py:232-242)
-  DV_TRY(dv_densities_factor(c, dst));  // compute_densities + compute_DFSPH_factor, one sweep
-  DV_TRY(dv_density_change(c, dst));
+  // compute_densities + compute_DFSPH_factor + the divergence solve's first
+  // compute_density_change, one sweep
+  DV_TRY(dv_densities_factor_change(c, dst));
   DV_TRY(dv_scale_factor(c, dst, c->p.inv_dt));
   DV_TRY(dv_batch_solve(c, dst, 0));
   DV_TRY(dv_scale_factor(c, dst, c->p.dt));

@@ -80,42 +80,60 @@ __global__ void k_dfsph_factor(dv_params P, DevGrid G, dv_fields F, const dv_cou
 // reference sweeps visit the same neighbours in the same order, and each sum
 // here is built by the same operations in that order, so density and factor
 // are bit-identical to k_densities and k_dfsph_factor; the list, position and
-// material of each neighbour are read once instead of twice.
-template <int D>
-__global__ void k_densities_factor(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+// material of each neighbour are read once instead of twice.  With DC the
+// same walk also does the compute_density_change that opens the divergence
+// solve (dimcv_sph.py:337-374): it reads only v, x and m_V, which neither of
+// the two sweeps changes, and shares their ∇W; density_adv is bit-identical
+// to k_density_change's.
+template <int D, bool DC>
+__device__ __forceinline__ void densities_factor_body(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                      const dv_counters* __restrict__ C) {
   FOR_I;
   if (F.material[i] != DV_MATERIAL_FLUID) return;
   V3 xi = ldv<D>(F.x, i);
+  V3 vi = DC ? ldv<D>(F.v, i) : V3{0.f, 0.f, 0.f};
   float dens = F.m_V[i] * cubic_W(P, 0.0f);
   float den = 0.0f;
   V3 gi{0.f, 0.f, 0.f};
   float sum_k = 0.0f;
+  float adv = 0.0f;
+  int nn = 0;
   for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
-    if (mj == DV_MATERIAL_FLUID) {
+    if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
       const float mvj = F.m_V[j];
       den += mvj * cubic_W(P, sqrtf(r2));
       V3 gw = cubic_gradW<D>(P, r, r2);
-      float mm = F.m[j];
-      V3 g{mm * gw.x, mm * gw.y, mm * gw.z};
-      sum_k += sqnorm<D>(g);
-      gi.x += g.x;
-      gi.y += g.y;
-      if (D == 3) gi.z += g.z;
-    } else if (mj == DV_MATERIAL_SOLID) {
-      const float mvj = F.m_V[j];
-      den += mvj * cubic_W(P, sqrtf(r2));
-      V3 gw = cubic_gradW<D>(P, r, r2);
-      float s = mvj * P.density0;
-      gi.x += s * gw.x;
-      gi.y += s * gw.y;
-      if (D == 3) gi.z += s * gw.z;
+      if (mj == DV_MATERIAL_FLUID) {
+        float mm = F.m[j];
+        V3 g{mm * gw.x, mm * gw.y, mm * gw.z};
+        sum_k += sqnorm<D>(g);
+        gi.x += g.x;
+        gi.y += g.y;
+        if (D == 3) gi.z += g.z;
+      } else {
+        float s = mvj * P.density0;
+        gi.x += s * gw.x;
+        gi.y += s * gw.y;
+        if (D == 3) gi.z += s * gw.z;
+      }
+      if (DC) {
+        V3 vj = ldv<D>(F.v, j);
+        V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+        adv += mvj * dot<D>(dv, gw);
+      }
     }
+    nn += 1;
   });
   dens += den;
   dens *= P.density0;
   F.density[i] = dens;
   sum_k += sqnorm<D>(gi);
   F.dfsph_factor[i] = sum_k > P.factor_min ? 1.0f / sum_k : 0.0f;
+  if (DC) {
+    float da = fmaxf(adv, 0.0f);
+    if (nn < P.neighbor_min) da = 0.0f;
+    F.density_adv[i] = da;
+  }
 }
 
 // multiply_time_step (dimcv_sph.py:395-399)
@@ -572,9 +590,24 @@ DV_API int dv_dfsph_factor(dv_ctx* c, const dv_fields* f) {
   return DV_OK;
 }
 
+template <int D>
+__global__ void k_densities_factor_only(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  densities_factor_body<D, false>(P, G, F, C);
+}
+template <int D>
+__global__ void k_densities_factor_change(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C) {
+  densities_factor_body<D, true>(P, G, F, C);
+}
+
 DV_API int dv_densities_factor(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_densities_factor, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  LAUNCH_D(k_densities_factor_only, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
+  return DV_OK;
+}
+
+DV_API int dv_densities_factor_change(dv_ctx* c, const dv_fields* f) {
+  if (!c || !f) return DV_EINVAL;
+  LAUNCH_D(k_densities_factor_change, nblk(c), c->p, dv_grid(c), *f, c->d_cnt);
   return DV_OK;
 }
 
@@ -751,9 +784,8 @@ static int read_iters(dv_ctx* c, int which, int32_t* iters) {
   return DV_OK;
 }
 
-DV_API int dv_divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
-  if (!c || !f) return DV_EINVAL;
-  int rc = dv_density_change(c, f);
+static int divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters, bool prepared) {
+  int rc = prepared ? DV_OK : dv_density_change(c, f);
   if (rc) return rc;
   rc = dv_scale_factor(c, f, c->p.inv_dt);
   if (rc) return rc;
@@ -762,6 +794,16 @@ DV_API int dv_divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
   rc = dv_scale_factor(c, f, c->p.dt);
   if (rc) return rc;
   return read_iters(c, 0, iters);
+}
+
+DV_API int dv_divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  return divergence_solve(c, f, iters, false);
+}
+
+DV_API int dv_divergence_solve_prepared(dv_ctx* c, const dv_fields* f, int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  return divergence_solve(c, f, iters, true);
 }
 
 DV_API int dv_pressure_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {

@@ -151,11 +151,13 @@ class DIMCVSPHSolver(SPHBase):
 
     # ----------------------------------------------------------- DFSPH
     # Sweeps that the reference runs back to back over the same neighbours
-    # are fused (dv_densities_factor, dv_vorticity_dvort): the first method
-    # computes both results and the second skips its sweep when no library
-    # kernel has run since, so nothing it reads can have changed through the
-    # library (a caller that edits the fields with torch in between calls the
-    # library entry point of the second sweep itself).
+    # are fused (dv_densities_factor_change, dv_vorticity_dvort): the first
+    # method computes all the results and the later ones skip their sweep
+    # when no library kernel has run since, so nothing it reads can have
+    # changed through the library (a caller that edits the fields with torch
+    # in between calls the library entry point of the later sweep itself).
+    # compute_densities thereby also writes density_adv, which the reference
+    # reads only after divergence_solve's own compute_density_change.
     _fused_factor_at = -1
     _fused_dvort_at = -1
 
@@ -167,8 +169,8 @@ class DIMCVSPHSolver(SPHBase):
             return  # computed by compute_densities' sweep, bit-identical
         self._call("dv_dfsph_factor")
 
-    def compute_densities(self):  # :139-148 (with :86-106 in the same sweep)
-        self._call("dv_densities_factor")
+    def compute_densities(self):  # :139-148 (with :86-106 and :337-358 in the same sweep)
+        self._call("dv_densities_factor_change")
         self._fused_factor_at = self._launches()
 
     def compute_non_pressure_forces(self):  # :195-208
@@ -181,6 +183,8 @@ class DIMCVSPHSolver(SPHBase):
         self._call("dv_predict_velocity")
 
     def compute_density_change(self):  # :337-358
+        if self._fused_factor_at == self._launches():
+            return  # computed by compute_densities' sweep, bit-identical
         self._call("dv_density_change")
 
     def multiply_time_step(self, field, time_step):  # :395-399
@@ -216,7 +220,9 @@ class DIMCVSPHSolver(SPHBase):
     def divergence_solve(self):
         """dimcv_sph.py:376-393, with the Jacobi loop on the device."""
         it = C.c_int32(0)
-        self._call("dv_divergence_solve", C.byref(it) if self.track_iterations else None)
+        fn = "dv_divergence_solve_prepared" if self._fused_factor_at == self._launches() \
+            else "dv_divergence_solve"
+        self._call(fn, C.byref(it) if self.track_iterations else None)
         self.last_iters = (it.value, self.last_iters[1])
 
     def pressure_solve(self):

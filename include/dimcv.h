@@ -279,6 +279,12 @@ DV_API int dv_dfsph_factor(dv_ctx* ctx, const dv_fields* f);
  * in one neighbour sweep: both fields bit-identical to dv_densities then
  * dv_dfsph_factor. */
 DV_API int dv_densities_factor(dv_ctx* ctx, const dv_fields* f);
+/* dv_densities_factor and, in the same neighbour sweep, the
+ * compute_density_change that opens divergence_solve (dimcv_sph.py:337-374,
+ * :377): density_adv bit-identical to dv_density_change's.  It reads v, x
+ * and m_V, which the two sweeps do not write; follow it with
+ * dv_divergence_solve_prepared while those are unchanged. */
+DV_API int dv_densities_factor_change(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.multiply_time_step(dfsph_factor, s) (dimcv_sph.py:395-399). */
 DV_API int dv_scale_factor(dv_ctx* ctx, const dv_fields* f, float s);
 /* DIMCVSPHSolver.compute_density_change (dimcv_sph.py:337-374). */
@@ -298,6 +304,10 @@ DV_API int dv_pressure_iteration(dv_ctx* ctx, const dv_fields* f);
  * host once per chunk of iterations.  *iters (host, may be NULL) receives
  * the iteration count (synchronises only if non-NULL). */
 DV_API int dv_divergence_solve(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
+/* dv_divergence_solve without its opening density change: density_adv must
+ * hold compute_density_change's result for the current v (from
+ * dv_densities_factor_change or dv_density_change). */
+DV_API int dv_divergence_solve_prepared(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
 /* DIMCVSPHSolver.pressure_solve (dimcv_sph.py:597-614), same loop form. */
 DV_API int dv_pressure_solve(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
 /* DIMCVSPHSolver.compute_non_pressure_forces (dimcv_sph.py:150-208). */

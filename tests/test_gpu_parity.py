@@ -445,8 +445,11 @@ def test_paired_fp32_far_loop_is_bit_identical_to_scalar(cuda, case):
 
 @pytest.mark.parametrize("scene", ["channel2d", "sphere3d_coarse"])
 def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
-    """dv_densities_factor, dv_vorticity_dvort and dv_smooth_akde give the
-    same bits as the pairs of sweeps they replace."""
+    """dv_densities_factor(_change), dv_vorticity_dvort and dv_smooth_akde
+    give the same bits as the sweeps they replace, and the divergence solve
+    that starts from the fused density change (the solver's own
+    compute_densities → compute_DFSPH_factor → divergence_solve) gives the
+    same velocities and iteration count as the unfused sequence."""
     cfg = scenes.channel2d(trim_cylinder=True) if scene == "channel2d" else scenes.sphere3d(radius=0.016)
     ps, solver = make(cfg)
     solver.initialize()
@@ -472,6 +475,41 @@ def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
     for k in a:
         bitexact(b[k], a[k], k)
     nontrivial(a["dfsph_factor"], "factor")
+
+    saved = {k: t.clone() for k, t in ps.fields.t.items()}
+    solver._call("dv_densities")
+    solver._call("dv_dfsph_factor")
+    solver._call("dv_density_change")
+    a = snap(["density", "dfsph_factor", "density_adv"])
+    for t in (ps.density, ps.dfsph_factor, ps.density_adv):
+        poison(t)
+    solver._call("dv_densities_factor_change")
+    b = snap(["density", "dfsph_factor", "density_adv"])
+    for k in a:
+        bitexact(b[k], a[k], k)
+    nontrivial(a["density_adv"], "density_adv")
+
+    import ctypes
+    solve = ["v", "density_adv", "dfsph_factor"]
+    for k, t in ps.fields.t.items():
+        t.copy_(saved[k])
+    it = ctypes.c_int32(0)
+    solver._call("dv_densities")
+    solver._call("dv_dfsph_factor")
+    solver._call("dv_divergence_solve", ctypes.byref(it))
+    a = snap(solve)
+    for k, t in ps.fields.t.items():
+        t.copy_(saved[k])
+    solver.track_iterations = True
+    launches = solver._launches()
+    solver.compute_densities()
+    solver.compute_DFSPH_factor()
+    assert solver._launches() == launches + 1  # one sweep for density, factor and density change
+    solver.divergence_solve()
+    b = snap(solve)
+    for k in solve:
+        bitexact(b[k], a[k], k)
+    assert solver.last_iters[0] == it.value >= 1
 
     names = ["solver.v_star", "vorticity", "solver.grad_v", "solver.d_vort"]
     solver._calls("dv_dimcv_vorticity")
