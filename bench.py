@@ -188,8 +188,9 @@ STAGES = {
 
 
 # Algorithmic HBM bytes per particle slot of each stage (3-D; 2-D uses d = 2
-# in the vector terms): every field a stage needs read once and every field
-# it produces written once, neighbour re-reads excluded.  Grid: x, keys and
+# in the vector terms): per sweep of the reference, every field it needs read
+# once and every field it produces written once, neighbour re-reads excluded
+# (a fused walk reads the fields its sweeps share once, so it moves fewer).  Grid: x, keys and
 # the permuted persistent set (96); DFSPH: densities 21, factor 25, density
 # change 33 (+ 57 + 33 per divergence iteration), non-pressure 41, predict 36,
 # density_adv 33 (+ 57 + 33 per pressure iteration); DIMCV: fused grad-v /
@@ -467,14 +468,17 @@ def run_ours(args, rank, world, local):
 def e2e(args, ps, solver, world):
     """The same metric through the public API (KarmanVortexSolver.step) with
     the state round-tripped through pinned host buffers every step: H2D of
-    x and v before the step, D2H of x and v after it, inside the timed region."""
+    x and v before the step, D2H of x and v after it, inside the timed region.
+    The host buffers have the reference's field shape, (capacity, dim) float32
+    (particle_system.py:153-154), and are copied through the ps.x / ps.v views
+    of the device's padded rows."""
     import torch
     cap = ps.particle_max_num
-    vs = ps.fields["x"].shape[1]
+    vs = ps.x.shape[1]
     hx = torch.empty((cap, vs), dtype=torch.float32, pin_memory=True)
     hv = torch.empty((cap, vs), dtype=torch.float32, pin_memory=True)
-    hx.copy_(ps.fields["x"])
-    hv.copy_(ps.fields["v"])
+    hx.copy_(ps.x)
+    hv.copy_(ps.v)
     torch.cuda.synchronize()
     steps = args.steps
     cnt0 = ps.counters()
@@ -482,11 +486,11 @@ def e2e(args, ps, solver, world):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
-        ps.fields["x"].copy_(hx, non_blocking=True)
-        ps.fields["v"].copy_(hv, non_blocking=True)
+        ps.x.copy_(hx, non_blocking=True)
+        ps.v.copy_(hv, non_blocking=True)
         solver.step()
-        hx.copy_(ps.fields["x"], non_blocking=True)
-        hv.copy_(ps.fields["v"], non_blocking=True)
+        hx.copy_(ps.x, non_blocking=True)
+        hv.copy_(ps.v, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
     barrier(world)
@@ -496,7 +500,8 @@ def e2e(args, ps, solver, world):
     nbytes = 2 * cap * vs * 4
     return {"value": world * n_fluid * steps / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
             "d2h_bytes_per_step": nbytes,
-            "api": "KarmanVortexSolver.step() with x, v copied from/to pinned host memory each step"}
+            "api": "KarmanVortexSolver.step() with x, v (capacity x dim float32 each, the reference's field "
+                   "shape) copied from/to pinned host memory each step"}
 
 
 # ----------------------------------------------------------- CPU baseline
