@@ -178,11 +178,22 @@ __global__ void k_batch_kden(dv_params P, dv_fields F, const float* __restrict__
 // target, sample and far-field tile offsets; M_s = max(1, floor(frac · fluid_s))
 // where the scene has targets with a positive kden_sum, else 0 (dv_sample).
 // One block; each thread owns a contiguous run of scenes.
+// Far-field blocks go out longest first: every block of scene s runs its
+// tile of targets over the scene's num_samples samples, so the scenes are
+// ranked by num_samples (descending, ties by scene index; scenes without
+// targets last), tile_off is assigned in rank order and order[r] is the scene
+// of rank r.  A block's sums depend only on its scene and tile, so the order
+// changes which blocks form the tail of the launch, not the results.  With
+// more than kOrderMax scenes the order is the scene order.
+constexpr int kOrderMax = 1024;
 __global__ void k_batch_offsets(dv_scene_state* st, int S, float frac, int tile_w, dv_counters* C,
-                                int32_t* misc) {
+                                int32_t* misc, int32_t* __restrict__ order) {
+  __shared__ int s_key[kOrderMax];
+  __shared__ int s_ord[kOrderMax];
+  const bool ranked = S <= kOrderMax;
   const int per = (S + blockDim.x - 1) / blockDim.x;
   const int s0 = min(S, (int)threadIdx.x * per), s1 = min(S, s0 + per);
-  int t = 0, m = 0, tiles = 0;
+  int t = 0, m = 0;
   for (int s = s0; s < s1; ++s) {
     const int nt = st[s].n_targets;
     int M = 0;
@@ -191,20 +202,38 @@ __global__ void k_batch_offsets(dv_scene_state* st, int S, float frac, int tile_
       if (M < 1) M = 1;
     }
     st[s].num_samples = M;
+    if (ranked) s_key[s] = nt > 0 ? M : -1;
     t += nt;
     m += M;
-    tiles += (nt + tile_w - 1) / tile_w;
   }
   int tt, mt, ct;
-  int ot = block_excl_scan(t, &tt);
+  int ot = block_excl_scan(t, &tt);  // its barriers publish s_key
   int om = block_excl_scan(m, &mt);
-  int oc = block_excl_scan(tiles, &ct);
   for (int s = s0; s < s1; ++s) {
     st[s].t_start = ot;
     st[s].m_off = om;
-    st[s].tile_off = oc;
     ot += st[s].n_targets;
     om += st[s].num_samples;
+  }
+  if (ranked) {
+    for (int s = s0; s < s1; ++s) {
+      const int k = s_key[s];
+      int r = 0;
+      for (int q = 0; q < S; ++q) {
+        const int kq = s_key[q];
+        r += (kq > k || (kq == k && q < s)) ? 1 : 0;
+      }
+      s_ord[r] = s;
+    }
+    __syncthreads();
+  }
+  int tiles = 0;
+  for (int r = s0; r < s1; ++r) tiles += (st[ranked ? s_ord[r] : r].n_targets + tile_w - 1) / tile_w;
+  int oc = block_excl_scan(tiles, &ct);
+  for (int r = s0; r < s1; ++r) {
+    const int s = ranked ? s_ord[r] : r;
+    st[s].tile_off = oc;
+    order[r] = s;
     oc += (st[s].n_targets + tile_w - 1) / tile_w;
   }
   if (threadIdx.x == 0) {
@@ -380,6 +409,7 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
   al((void**)&b->d_wl, sizeof(int32_t) * (n_scenes + 1));
   al((void**)&b->d_ctr, sizeof(int32_t));
   al((void**)&b->d_misc, sizeof(int32_t) * 4);
+  al((void**)&b->d_order, sizeof(int32_t) * n_scenes);
   al((void**)&b->d_err, sizeof(double) * c->cap);
   al((void**)&b->d_step, sizeof(int64_t));
   al((void**)&b->d_emit, sizeof(float) * c->p.dim * std::max(n_emit, 1));
@@ -391,6 +421,7 @@ DV_API int dv_batch_setup(dv_ctx* c, const dv_batch_scene* scenes, int32_t n_sce
   if (e == cudaSuccess) e = cudaMemset(b->d_state, 0, sizeof(dv_scene_state) * n_scenes);
   if (e == cudaSuccess) e = cudaMemset(b->d_done, 0, sizeof(int32_t) * (n_scenes + 1));
   if (e == cudaSuccess) e = cudaMemset(b->d_misc, 0, sizeof(int32_t) * 4);
+  if (e == cudaSuccess) e = cudaMemset(b->d_order, 0, sizeof(int32_t) * n_scenes);
   if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(double) * c->cap);
   if (e == cudaSuccess) e = cudaMemset(b->d_step, 0, sizeof(int64_t));
   if (e == cudaSuccess && n_emit > 0)
@@ -424,6 +455,7 @@ void dv_batch_free(dv_ctx* c) {
   cudaFree(b->d_wl);
   cudaFree(b->d_ctr);
   cudaFree(b->d_misc);
+  cudaFree(b->d_order);
   cudaFree(b->d_err);
   cudaFree(b->d_step);
   cudaFree(b->d_emit);
@@ -484,7 +516,7 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
     k_batch_kden<3><<<S, 1024, 0, c->stream>>>(c->p, *dst, s->kden, b->d_state);
   DV_LAUNCHED(c);
   k_batch_offsets<<<1, 1024, 0, c->stream>>>(b->d_state, S, b->mc_fraction, dv_far_tile_width(c), c->d_cnt,
-                                             b->d_misc);
+                                             b->d_misc, b->d_order);
   DV_LAUNCHED(c);
   DV_TRY(dv_build_targets(c, dst));
   DV_TRY(dv_batch_draw(c, s));

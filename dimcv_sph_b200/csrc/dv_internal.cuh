@@ -155,6 +155,7 @@ struct dv_batch_state {
   int32_t* d_wl = nullptr;            // [S + 1]: work list of the scenes still iterating (block offsets)
   int32_t* d_ctr = nullptr;           // iterations of the captured Jacobi loop
   int32_t* d_misc = nullptr;          // [0]: far-field tiles this step
+  int32_t* d_order = nullptr;         // [S]: scenes in far-field block order (most samples per tile first)
   double* d_err = nullptr;            // [cap] residual block sums of the solves (one per work-list block)
   int64_t* d_step = nullptr;          // step counter (emission schedule, sampler stream)
   float* d_emit = nullptr;            // [n_emit][dim]

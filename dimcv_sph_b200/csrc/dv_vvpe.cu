@@ -567,31 +567,40 @@ __global__ void k_far_fix_b(dv_params P, DevGrid G, dv_fields F, dv_solver_field
                               (uint32_t)sc << G.scene_shift, mult, srank, sslot, far_acc, near_v, near_S, 1, 0);
 }
 
-// scene batch main loop: block b is tile b - tile_off_s of the scene s with
-// tile_off_s <= b; its targets [t_start_s + tile·FT2·TT, ...) of the scene
-// run over the scene's samples [m_off_s, m_off_s + M_s) in the order and
-// tiling of k_far_main
+// scene of far-field block blk: the last scene in block order whose first
+// block is at or before blk (tile_off increases along order[], one or more
+// blocks per scene with targets)
+__device__ __forceinline__ int batch_block_scene(const dv_scene_state* __restrict__ st,
+                                                 const int32_t* __restrict__ order, int S, int blk) {
+  int lo = 0, hi = S;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (st[order[mid]].tile_off <= blk)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return order[lo - 1];
+}
+
+// scene batch main loop: block b is tile b - tile_off_s of its scene s
+// (batch_block_scene); its targets [t_start_s + tile·FT2·TT, ...) of the
+// scene run over the scene's samples [m_off_s, m_off_s + M_s) in the order
+// and tiling of k_far_main
 template <int D, int TT, bool BLOB, bool COMP>
 __global__ void __launch_bounds__(FT2) k_far_main_b(dv_params P, const float* __restrict__ x,
                                                     const int32_t* __restrict__ targets,
                                                     const float4* __restrict__ spos,
                                                     const float4* __restrict__ sw,
-                                                    const dv_scene_state* __restrict__ st, int S,
+                                                    const dv_scene_state* __restrict__ st,
+                                                    const int32_t* __restrict__ order, int S,
                                                     const int32_t* __restrict__ ntiles,
                                                     float4* __restrict__ far_acc) {
   __shared__ float4 s_p[FTILE2];
   __shared__ float4 s_w[FTILE2];
   const int blk = blockIdx.x;
   if (blk >= *ntiles) return;  // uniform per CTA
-  int lo = 0, hi = S;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (st[mid].tile_off <= blk)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  const int sc = lo - 1;
+  const int sc = batch_block_scene(st, order, S, blk);
   const int t0 = st[sc].t_start, nt = st[sc].n_targets;
   const int m0 = st[sc].m_off, M = st[sc].num_samples;
   const int tbase = (blk - st[sc].tile_off) * FT2 * TT;
@@ -828,21 +837,14 @@ __global__ void __launch_bounds__(FT2, DV_FAR_MINB(TT)) k_far_main_x2_b(dv_param
                                                        const int32_t* __restrict__ targets,
                                                        const float4* __restrict__ spos,
                                                        const float4* __restrict__ sw,
-                                                       const dv_scene_state* __restrict__ st, int S,
+                                                       const dv_scene_state* __restrict__ st,
+                                                       const int32_t* __restrict__ order, int S,
                                                        const int32_t* __restrict__ ntiles,
                                                        float4* __restrict__ far_acc) {
   __shared__ float4 s4[(D == 3 ? 4 : 2) * FTILE2];
   const int blk = blockIdx.x;
   if (blk >= *ntiles) return;  // uniform per CTA
-  int lo = 0, hi = S;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (st[mid].tile_off <= blk)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  const int sc = lo - 1;
+  const int sc = batch_block_scene(st, order, S, blk);
   const int t0 = st[sc].t_start;
   far_x2_run<D, TT>(P, x, targets + t0, st[sc].n_targets, (blk - st[sc].tile_off) * FT2 * TT, spos, sw,
                     st[sc].m_off, st[sc].num_samples, far_acc + t0, s4);
@@ -1106,10 +1108,10 @@ static void launch_main_b(dv_ctx* c, const dv_fields* f) {
   const int nb = (int)b->cap_tiles;
 #define L(TTV)                                                                                             \
   k_far_main_b<D, TTV, BLOB, COMP><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw,      \
-                                                              b->d_state, b->S, b->d_misc, c->far_acc)
+                                                              b->d_state, b->d_order, b->S, b->d_misc, c->far_acc)
 #define L2(TTV)                                                                                            \
   k_far_main_x2_b<D, TTV><<<nb, FT2, 0, c->stream>>>(c->p, f->x, c->targets, c->spos, c->sw, b->d_state,    \
-                                                     b->S, b->d_misc, c->far_acc)
+                                                     b->d_order, b->S, b->d_misc, c->far_acc)
   constexpr bool paired = !BLOB && !COMP;
   const int tt = far_tile_run(c->far_tt, paired);  // as dv_far_tile_width, which sized the tiles
   if (tt == 2) {

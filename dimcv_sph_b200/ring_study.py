@@ -60,9 +60,13 @@ class RingStudy:
         ps.params.compensated = 1 if on else 0
         _lib.check(ps.ctx, ps.lib.dv_set_params(ps.ctx, C.byref(ps.params)), "dv_set_params")
 
-    def mc_step(self, M: int, seed_step: int, mode: int = DV_SAMPLE_INVERSE_CDF):
+    def mc_step(self, M: int, seed_step: int, mode: int = DV_SAMPLE_INVERSE_CDF, restore: bool = True):
+        """One MC-VVPE step from the ring's initial velocity (restore) or from
+        the velocity the last step left; the work of a step (pairs, sweeps)
+        does not depend on which, so the timings skip the restore."""
         ps, s = self.ps, self.solver
-        ps.v[: self.n] = self.v0
+        if restore:
+            ps.v[: self.n] = self.v0
         ps.initialize_particle_system()
         s._calls("dv_dimcv_vorticity")  # ∇v for KVN (the step's Δω is not used here)
         s.compute_kinematic_vorticity_num_sample()
@@ -91,8 +95,8 @@ class RingStudy:
         return e0.elapsed_time(e1) / reps
 
 
-def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=8, subset=262144, reps=3, target_err=0.02,
-        device="cuda") -> dict:
+def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 51200, 53248, 57344, 65536, 131072), seeds=8,
+        subset=262144, reps=3, target_err=0.02, tune_M=49152, device="cuda") -> dict:
     st = RingStudy(n=n, subset=subset, device=device)
     out = {"n": n, "subset": int(st.sub.numel()), "kernel": "blob3d (1/4π) V (r×ω)/(|r|²+δ²)^{3/2}, δ = r",
            "bs_f32_vs_f64": {}, "mc": []}
@@ -118,13 +122,20 @@ def run(n=1 << 20, Ms=(4096, 16384, 32768, 40960, 49152, 65536, 131072), seeds=8
     out["bs_tile_sweep_ms"] = {str(k): v for k, v in tiles.items()}
     out["bs_particle_steps_per_s"] = n / (bs_ms * 1e-3)
     out["bs_tflops_incl_grid"] = 27.0 * n * (n - 1) / (bs_ms * 1e-3) / 1e12
+    # the MC steps' far tile: the autotuner's choice at tune_M samples, near
+    # the matched error, instead of at the first M of the sweep
+    st.solver.far_tile = None
+    st.mc_step(tune_M, 999, DV_SAMPLE_STRATIFIED)
+    out["mc_far_tile"] = st.solver.far_tile
+    out["mc_far_tile_tuned_at_M"] = tune_M
     for mode_name, mode in (("iid", DV_SAMPLE_INVERSE_CDF), ("stratified", DV_SAMPLE_STRATIFIED)):
         for M in Ms:
             errs = []
             for k in range(seeds):
                 st.mc_step(M, 1000 + k, mode)
                 errs.append(st.mc_error())
-            ms = st.timed(lambda: st.mc_step(M, 7, mode), reps)
+            st.mc_step(M, 7, mode)
+            ms = st.timed(lambda: st.mc_step(M, 7, mode, restore=False), reps)
             st.set_compensated(True)
             st.mc_step(M, 1000, mode)
             err_comp = st.mc_error()

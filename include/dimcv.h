@@ -518,7 +518,7 @@ typedef struct dv_scene_state {  /* per scene, device-resident; read with dv_bat
   int32_t n_fluid, n_solid;
   int32_t t_start, n_targets;    /* range in the target list */
   int32_t m_off, num_samples;    /* range in sample_idx */
-  int32_t tile_off, iters_div;
+  int32_t tile_off, iters_div;  /* tile_off: first far-field block of the scene (blocks go out most samples first) */
   int32_t iters_p, done;
   int32_t status, emitted;       /* DV_WARN_* bits of the scene; particles emitted so far */
   double err_div, err_p, kden_sum;
