@@ -152,26 +152,41 @@ class DIMCVSPHSolver(SPHBase):
     # ----------------------------------------------------------- DFSPH
     # Sweeps that the reference runs back to back over the same neighbours
     # are fused (dv_densities_factor_change, dv_vorticity_dvort): the first
-    # method computes all the results and the later ones skip their sweep
-    # when no library kernel has run since, so nothing it reads can have
-    # changed through the library (a caller that edits the fields with torch
-    # in between calls the library entry point of the later sweep itself).
+    # method computes all the results and a later one skips its sweep while
+    # nothing it reads can have changed: no library kernel has run since
+    # (the context's launch count) and no tensor it reads was written in place
+    # by torch (the tensors' version counters, which views share).
     # compute_densities thereby also writes density_adv, which the reference
     # reads only after divergence_solve's own compute_density_change.
-    _fused_factor_at = -1
-    _fused_dvort_at = -1
+    _FACTOR_READS = ("x", "m", "m_V", "material")          # compute_DFSPH_factor
+    _CHANGE_READS = ("x", "v", "m_V", "material")          # compute_density_change
+    _DVORT_READS = ("x", "m_V", "material", "vorticity")   # compute_d_vorticity, with v_star
+    _fused_densities = None
+    _fused_dvort = None
 
     def _launches(self):
         return self.lib.dv_launch_count(self.ctx)
 
+    def _fusion_mark(self, names, solver_names=()):
+        f, sb = self.ps.fields, self._sb
+        return {"at": self._launches(), "set": f,
+                "ver": {**{n: f[n]._version for n in names}, **{"sb." + n: sb[n]._version for n in solver_names}}}
+
+    def _fusion_fresh(self, mark, names, solver_names=()) -> bool:
+        if mark is None or mark["at"] != self._launches() or mark["set"] is not self.ps.fields:
+            return False
+        f, sb, ver = self.ps.fields, self._sb, mark["ver"]
+        return all(f[n]._version == ver[n] for n in names) and \
+            all(sb[n]._version == ver["sb." + n] for n in solver_names)
+
     def compute_DFSPH_factor(self):  # dimcv_sph.py:86-106
-        if self._fused_factor_at == self._launches():
+        if self._fusion_fresh(self._fused_densities, self._FACTOR_READS):
             return  # computed by compute_densities' sweep, bit-identical
         self._call("dv_dfsph_factor")
 
     def compute_densities(self):  # :139-148 (with :86-106 and :337-358 in the same sweep)
         self._call("dv_densities_factor_change")
-        self._fused_factor_at = self._launches()
+        self._fused_densities = self._fusion_mark(set(self._FACTOR_READS) | set(self._CHANGE_READS))
 
     def compute_non_pressure_forces(self):  # :195-208
         self._call("dv_nonpressure")
@@ -183,7 +198,7 @@ class DIMCVSPHSolver(SPHBase):
         self._call("dv_predict_velocity")
 
     def compute_density_change(self):  # :337-358
-        if self._fused_factor_at == self._launches():
+        if self._fusion_fresh(self._fused_densities, self._CHANGE_READS):
             return  # computed by compute_densities' sweep, bit-identical
         self._call("dv_density_change")
 
@@ -220,7 +235,7 @@ class DIMCVSPHSolver(SPHBase):
     def divergence_solve(self):
         """dimcv_sph.py:376-393, with the Jacobi loop on the device."""
         it = C.c_int32(0)
-        fn = "dv_divergence_solve_prepared" if self._fused_factor_at == self._launches() \
+        fn = "dv_divergence_solve_prepared" if self._fusion_fresh(self._fused_densities, self._CHANGE_READS) \
             else "dv_divergence_solve"
         self._call(fn, C.byref(it) if self.track_iterations else None)
         self.last_iters = (it.value, self.last_iters[1])
@@ -245,10 +260,10 @@ class DIMCVSPHSolver(SPHBase):
 
     def init(self):  # :803-806 — one sweep for v*, ω and ∇v, and Δω (:573-583) with them
         self._calls("dv_vorticity_dvort")
-        self._fused_dvort_at = self._launches()
+        self._fused_dvort = self._fusion_mark(self._DVORT_READS, ("v_star",))
 
     def compute_d_vorticity(self):  # :573-583
-        if self._fused_dvort_at == self._launches():
+        if self._fusion_fresh(self._fused_dvort, self._DVORT_READS, ("v_star",)):
             return  # computed by init's sweep, bit-identical
         self._calls("dv_d_vorticity")
 

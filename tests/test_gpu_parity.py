@@ -538,3 +538,62 @@ def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
         bitexact(b[k], a[k], k)
     assert ps.counters()["kden_sum"] == ka
     nontrivial(a["solver.kden"], "kden")
+
+
+def test_fused_skips_follow_torch_edits(cuda):
+    """A sweep fused into an earlier one is skipped only while nothing it reads
+    has changed: an in-place torch edit of v between compute_densities and
+    divergence_solve, or of x before compute_DFSPH_factor, makes the solver
+    run the sweep itself, with the results of the unfused sequence."""
+    import ctypes
+    ps, solver = make(scenes.channel2d(trim_cylinder=True))
+    solver.initialize()
+    solver._call("dv_nonpressure")
+    n = ps.particle_num[None]
+    saved = {k: t.clone() for k, t in ps.fields.t.items()}
+
+    def restore():
+        for k, t in ps.fields.t.items():
+            t.copy_(saved[k])
+
+    def snap(names):
+        g = ps.snapshot()
+        return {k: g[k].copy() for k in names}
+
+    solve = ["v", "density_adv", "dfsph_factor"]
+    it = ctypes.c_int32(0)
+    solver._call("dv_densities")
+    solver._call("dv_dfsph_factor")
+    ps.v[:n] *= 1.5
+    solver._call("dv_divergence_solve", ctypes.byref(it))
+    a = snap(solve)
+
+    restore()
+    solver.compute_densities()
+    ps.v[:n] *= 1.5
+    stale = ctypes.c_int32(0)
+    solver._call("dv_divergence_solve_prepared", ctypes.byref(stale))
+    s = snap(["v"])
+    assert not np.array_equal(s["v"], a["v"])  # the pre-edit density change gives another answer
+
+    restore()
+    solver.track_iterations = True
+    solver.compute_densities()
+    solver.compute_DFSPH_factor()  # reads no v: still the fused result
+    ps.v[:n] *= 1.5
+    solver.divergence_solve()
+    b = snap(solve)
+    for k in solve:
+        bitexact(b[k], a[k], k)
+    assert solver.last_iters[0] == it.value
+
+    restore()
+    solver._call("dv_densities")
+    ps.x[:n] += 1e-4
+    solver._call("dv_dfsph_factor")
+    a = snap(["dfsph_factor"])
+    restore()
+    solver.compute_densities()
+    ps.x[:n] += 1e-4
+    solver.compute_DFSPH_factor()
+    bitexact(snap(["dfsph_factor"])["dfsph_factor"], a["dfsph_factor"], "dfsph_factor")
