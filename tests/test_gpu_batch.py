@@ -133,3 +133,23 @@ def test_one_scene_batch_is_the_lone_run_in_a_graph(small):
     fg, fe = g.scene_fields(0, FIELDS, sg), e.scene_fields(0, FIELDS, se)
     for k in FIELDS:
         assert np.array_equal(fg[k], fe[k]), k
+
+
+def test_more_scenes_than_the_ranked_block_order(cuda):
+    """1,030 scenes, more than the 1,024 whose far-field blocks are issued
+    longest first: the batch falls back to scene order, and scenes at both
+    ends and in the middle still equal their lone runs."""
+    from dimcv_sph_b200.batch import SceneBatch, channel_batch_configs
+    cfgs, _ = channel_batch_configs(n_scenes=1030, seed=5, n_min=300, n_max=800, reserve_steps=20)
+    b = SceneBatch(cfgs, keep_snapshots=True)
+    steps = 2
+    for _ in range(steps):
+        b.step()
+    st = b.states()
+    for s in (0, 515, 1029):
+        ps, sv = lone_run(cfgs[s], b.grid_num, b.snaps[s], b.snap_counts[s], steps)
+        c = ps.counters()
+        assert st[s]["end"] - st[s]["start"] == c["n"] and st[s]["num_samples"] == c["num_samples"], s
+        got = b.scene_fields(s, FIELDS, st)
+        for k in FIELDS:
+            assert np.array_equal(got[k], ps.fields[k][: c["n"]].cpu().numpy()), (s, k)
