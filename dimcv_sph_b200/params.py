@@ -83,8 +83,14 @@ class Options:
 
 
 def make_params(cfg, options: Options | None = None) -> DvParams:
-    o = options or Options.from_config(cfg)
     g = cfg.get_cfg
+    if g("domainStart") is None or g("domainEnd") is None:
+        seg = " (a SegmentConfiguration scene of the reference's vortex-segment solver, " \
+              "run_segment_simulation.py, which this library does not implement)" \
+            if "SegmentConfiguration" in getattr(cfg, "config", {}) else ""
+        raise ValueError("the scene has no Configuration.domainStart / domainEnd, which the SPH particle "
+                         f"system needs (particle_system.py:17-20){seg}")
+    o = options or Options.from_config(cfg)
     domain_start = np.array(g("domainStart"), dtype=np.float64)  # particle_system.py:17
     domain_end = np.array(g("domainEnd"), dtype=np.float64)      # :20
     domain_size = domain_end - domain_start                      # :22

@@ -115,3 +115,14 @@ def test_channel_batch_configs():
         assert g("computeVis") is False and g("samplerMode") == "inverse_cdf"
     # the shared batch grid is the largest scene grid
     assert np.all(grids.max(axis=0) >= grids)
+
+
+def test_scene_without_a_domain_is_a_clear_error():
+    """A scene of the reference's vortex-segment solver (SegmentConfiguration,
+    no Configuration.domainStart) is refused with a message, not a TypeError."""
+    import pytest
+    from dimcv_sph_b200.config_builder import SimConfig
+    cfg = SimConfig(config={"Configuration": {"particleRadius": 0.01, "timeStep": 0.002},
+                            "SegmentConfiguration": {"initType": "v_bundle_pair"}})
+    with pytest.raises(ValueError, match="segment"):
+        make_params(cfg)
