@@ -26,6 +26,9 @@ DV_SAMPLE_INVERSE_CDF = 1
 DV_SAMPLE_INJECTED = 2
 DV_SAMPLE_STRATIFIED = 3
 
+DV_SOLVE_PREPARED = 1
+DV_SOLVE_NONPRESSURE = 2
+
 DV_KERNEL_REF2D = 0
 DV_KERNEL_BLOB3D = 1
 

@@ -50,6 +50,7 @@ PROTOTYPES = {
     "dv_pressure_iteration": (C.c_int, [_P, _FP]),
     "dv_divergence_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_divergence_solve_prepared": (C.c_int, [_P, _FP, C.POINTER(i32)]),
+    "dv_divergence_solve_ex": (C.c_int, [_P, _FP, i32, C.POINTER(i32)]),
     "dv_pressure_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_nonpressure": (C.c_int, [_P, _FP]),
     "dv_predict_velocity": (C.c_int, [_P, _FP]),

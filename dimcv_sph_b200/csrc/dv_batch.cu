@@ -502,9 +502,11 @@ DV_API int dv_batch_step(dv_ctx* c, const dv_fields* src, const dv_fields* dst, 
   // compute_density_change, one sweep
   DV_TRY(dv_densities_factor_change(c, dst));
   DV_TRY(dv_scale_factor(c, dst, c->p.inv_dt));
-  DV_TRY(dv_batch_solve(c, dst, 0));
+  // the divergence loop's last residual sweep also gives the non-pressure
+  // forces of the solved velocity; a loop of no iterations runs that sweep
+  DV_TRY(dv_batch_solve(c, dst, 0, true));
+  if (c->p.max_iter_div < 1) DV_TRY(dv_nonpressure(c, dst));
   DV_TRY(dv_scale_factor(c, dst, c->p.dt));
-  DV_TRY(dv_nonpressure(c, dst));
   // v*, ω, ∇v and Δω in one sweep; KVN (independent of the smoothing) before
   // the sweep that smooths Δω and sums the AKDE
   DV_TRY(dv_vorticity_dvort(c, dst, s));

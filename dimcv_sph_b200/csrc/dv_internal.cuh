@@ -175,7 +175,9 @@ int dv_batch_solve_reset(dv_ctx* c, int which);
 int dv_batch_solve_finalize(dv_ctx* c, int which);
 int dv_batch_loop_condition(dv_ctx* c, cudaGraphConditionalHandle h, int max_iter);
 // dv_sph.cu: one DFSPH Jacobi solve with per-scene convergence
-int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which);
+// which 0 (divergence) or 1 (pressure); nonpressure: the divergence residual
+// sweeps also compute compute_non_pressure_forces (as DV_SOLVE_NONPRESSURE)
+int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which, bool nonpressure = false);
 // dv_dimcv.cu: per-scene inverse-CDF draws (targets built)
 int dv_batch_draw(dv_ctx* c, const dv_solver_fields* s);
 // dv_vvpe.cu: near field, far field (scene targets x scene samples), gate

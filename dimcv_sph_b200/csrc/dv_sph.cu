@@ -168,6 +168,53 @@ __device__ __forceinline__ double density_change_one(const dv_params& P, const D
   return (double)term;
 }
 
+// density_change_one and, in the same walk, compute_non_pressure_forces
+// (dimcv_sph.py:150-208) of slot i: the fluid neighbours' viscosity term
+// takes v_i - v_j, ∇W and m_V_j from the density change and adds up in the
+// visit order with the operations of k_nonpressure, so the acceleration is
+// bit-identical to k_nonpressure's for the same v.  Every slot gets its
+// acceleration as k_nonpressure writes it (static solids 0, other non-fluid
+// slots gravity).
+template <int D>
+__device__ __forceinline__ double density_change_np_one(const dv_params& P, const DevGrid& G, const dv_fields& F,
+                                                        int i) {
+  const int mi = F.material[i];
+  const V3 g{P.gravity[0], P.gravity[1], D == 3 ? P.gravity[2] : 0.0f};
+  if (mi != DV_MATERIAL_FLUID) {
+    stv<D>(F.acceleration, i, (mi == DV_MATERIAL_SOLID && !F.is_dynamic[i]) ? V3{0.f, 0.f, 0.f} : g);
+    return 0.0;
+  }
+  V3 xi = ldv<D>(F.x, i);
+  V3 vi = ldv<D>(F.v, i);
+  float adv = 0.0f;
+  int nn = 0;
+  V3 acc = g;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    if (mj == DV_MATERIAL_FLUID || mj == DV_MATERIAL_SOLID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      const float mvj = F.m_V[j];
+      V3 gw = cubic_gradW<D>(P, r, r2);
+      adv += mvj * dot<D>(dv, gw);
+      if (mj == DV_MATERIAL_FLUID) {
+        float v_xy = dot<D>(dv, r);
+        float rn = sqrtf(r2);
+        float s = P.visc_coef * mvj * v_xy / (rn * rn + P.visc_h2);
+        acc.x += s * gw.x;
+        acc.y += s * gw.y;
+        if (D == 3) acc.z += s * gw.z;
+      }
+    }
+    nn += 1;
+  });
+  stv<D>(F.acceleration, i, acc);
+  float da = fmaxf(adv, 0.0f);
+  if (nn < P.neighbor_min) da = 0.0f;
+  F.density_adv[i] = da;
+  float term = P.has_transit ? transit_weight(P, xi.x) * (da - 0.0f) : (da - 0.0f);
+  return (double)term;
+}
+
 // optionally the FP64 block partial of the error terms
 template <int D>
 __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
@@ -180,6 +227,18 @@ __global__ void k_density_change(dv_params P, DevGrid G, dv_fields F, const dv_c
     double s = block_sum<double>(err);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
   }
+}
+
+// the divergence Jacobi loop's residual sweep with the non-pressure forces
+template <int D>
+__global__ void k_density_change_np(dv_params P, DevGrid G, dv_fields F, const dv_counters* __restrict__ C,
+                                    const int32_t* __restrict__ done, double* __restrict__ part) {
+  if (*done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (i < C->n) err = density_change_np_one<D>(P, G, F, i);
+  double s = block_sum<double>(err);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
 // ------------------------------------------------------------ density adv
@@ -422,7 +481,8 @@ __global__ void k_batch_iter(dv_params P, DevGrid G, dv_fields F, const dv_scene
 }
 
 // residual sweep: FP64 block sum of the error terms of work-list block b
-// (a block never spans two scenes) into part[b]
+// (a block never spans two scenes) into part[b]; WHICH 2 is the divergence
+// residual with the non-pressure forces (density_change_np_one)
 template <int D, int WHICH>
 __global__ void k_batch_residual(dv_params P, DevGrid G, dv_fields F, const dv_scene_state* __restrict__ st,
                                  const int32_t* __restrict__ wl, int S, double* __restrict__ part) {
@@ -431,7 +491,10 @@ __global__ void k_batch_residual(dv_params P, DevGrid G, dv_fields F, const dv_s
     const int s = wl_scene(wl, S, b);
     const int i = st[s].start + (b - wl[s]) * DV_THREADS + threadIdx.x;
     double e = 0.0;
-    if (i < st[s].end) e = WHICH == 0 ? density_change_one<D>(P, G, F, i) : density_adv_one<D>(P, G, F, i);
+    if (i < st[s].end)
+      e = WHICH == 0   ? density_change_one<D>(P, G, F, i)
+          : WHICH == 1 ? density_adv_one<D>(P, G, F, i)
+                       : density_change_np_one<D>(P, G, F, i);
     e = block_sum<double>(e);
     if (threadIdx.x == 0) part[b] = e;
   }
@@ -660,7 +723,7 @@ DV_API int dv_pressure_iteration(dv_ctx* c, const dv_fields* f) {
 // Runs Jacobi iterations in chunks of 2, 4, 8, ... launches; every iteration
 // is (update sweep, residual sweep + FP64 block partials, finalize) and all
 // three return at once once the done flag is set.
-static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
+static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which, bool nonpressure = false) {
   const int nb = nblk(c);
   const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
   const double eta = which == 0 ? c->p.eta_div : c->p.eta_p;
@@ -673,8 +736,12 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
     for (int k = 0; k < m; ++k) {
       if (which == 0) {
         LAUNCH_D(k_divergence_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
-        LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
-                 c->red_part);
+        if (nonpressure)
+          LAUNCH_D(k_density_change_np, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                   c->red_part);
+        else
+          LAUNCH_D(k_density_change, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done,
+                   c->red_part);
       } else {
         LAUNCH_D(k_pressure_iter, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
         if (c->dyn_rigid) LAUNCH_D(k_rigid_reaction, nb, c->p, dv_grid(c), *f, c->d_cnt, (const int32_t*)done);
@@ -702,7 +769,7 @@ static int jacobi_loop(dv_ctx* c, const dv_fields* f, int which) {
 // a conditional WHILE node whose condition kernel counts its own iterations
 // and stops at max_iter whatever the data, or earlier when every scene has
 // converged.
-static int batch_iteration(dv_ctx* c, const dv_fields* f, int which) {
+static int batch_iteration(dv_ctx* c, const dv_fields* f, int which, bool nonpressure) {
   dv_batch_state* b = c->batch;
   const int grid = c->num_sms * 8;
   const DevGrid G = dv_grid(c);
@@ -717,12 +784,20 @@ static int batch_iteration(dv_ctx* c, const dv_fields* f, int which) {
     DV_LAUNCHED(c);                                                                          \
   } while (0)
   LB(k_batch_iter, c->p, G, *f, b->d_state, b->d_wl, b->S);
-  LB(k_batch_residual, c->p, G, *f, b->d_state, b->d_wl, b->S, b->d_err);
+  if (which == 0 && nonpressure) {
+    if (c->p.dim == 2)
+      k_batch_residual<2, 2><<<grid, DV_THREADS, 0, c->stream>>>(c->p, G, *f, b->d_state, b->d_wl, b->S, b->d_err);
+    else
+      k_batch_residual<3, 2><<<grid, DV_THREADS, 0, c->stream>>>(c->p, G, *f, b->d_state, b->d_wl, b->S, b->d_err);
+    DV_LAUNCHED(c);
+  } else {
+    LB(k_batch_residual, c->p, G, *f, b->d_state, b->d_wl, b->S, b->d_err);
+  }
 #undef LB
   return dv_batch_solve_finalize(c, which);
 }
 
-int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which) {
+int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which, bool nonpressure) {
   dv_batch_state* b = c->batch;
   const int max_iter = which == 0 ? c->p.max_iter_div : c->p.max_iter_p;
   int rc = dv_batch_solve_reset(c, which);
@@ -749,7 +824,7 @@ int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which) {
     DV_CK(c, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     DV_CK(c, cudaStreamBeginCaptureToGraph(b->bstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     c->stream = b->bstream;
-    rc = batch_iteration(c, f, which);
+    rc = batch_iteration(c, f, which, nonpressure);
     if (rc == DV_OK) rc = dv_batch_loop_condition(c, h, max_iter);
     c->stream = st;
     cudaGraph_t out = nullptr;
@@ -762,7 +837,7 @@ int dv_batch_solve(dv_ctx* c, const dv_fields* f, int which) {
   while (launched < max_iter) {
     const int m = std::min(chunk, max_iter - launched);
     for (int k = 0; k < m; ++k) {
-      rc = batch_iteration(c, f, which);
+      rc = batch_iteration(c, f, which, nonpressure);
       if (rc) return rc;
     }
     launched += m;
@@ -784,13 +859,22 @@ static int read_iters(dv_ctx* c, int which, int32_t* iters) {
   return DV_OK;
 }
 
-static int divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters, bool prepared) {
-  int rc = prepared ? DV_OK : dv_density_change(c, f);
+// the residual sweep after the last iteration sees the solved velocity, and
+// nothing writes v after it: with DV_SOLVE_NONPRESSURE that sweep's
+// accelerations are compute_non_pressure_forces of the result (a loop of no
+// iterations runs the sweep itself)
+static int divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters, int32_t flags) {
+  const bool nonpressure = (flags & DV_SOLVE_NONPRESSURE) != 0;
+  int rc = (flags & DV_SOLVE_PREPARED) ? DV_OK : dv_density_change(c, f);
   if (rc) return rc;
   rc = dv_scale_factor(c, f, c->p.inv_dt);
   if (rc) return rc;
-  rc = jacobi_loop(c, f, 0);
+  rc = jacobi_loop(c, f, 0, nonpressure);
   if (rc) return rc;
+  if (nonpressure && c->p.max_iter_div < 1) {
+    rc = dv_nonpressure(c, f);
+    if (rc) return rc;
+  }
   rc = dv_scale_factor(c, f, c->p.dt);
   if (rc) return rc;
   return read_iters(c, 0, iters);
@@ -798,12 +882,19 @@ static int divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters, bool 
 
 DV_API int dv_divergence_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {
   if (!c || !f) return DV_EINVAL;
-  return divergence_solve(c, f, iters, false);
+  return divergence_solve(c, f, iters, 0);
 }
 
 DV_API int dv_divergence_solve_prepared(dv_ctx* c, const dv_fields* f, int32_t* iters) {
   if (!c || !f) return DV_EINVAL;
-  return divergence_solve(c, f, iters, true);
+  return divergence_solve(c, f, iters, DV_SOLVE_PREPARED);
+}
+
+DV_API int dv_divergence_solve_ex(dv_ctx* c, const dv_fields* f, int32_t flags, int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  if (flags & ~(DV_SOLVE_PREPARED | DV_SOLVE_NONPRESSURE))
+    return dv_fail(c, DV_EINVAL, "dv_divergence_solve_ex: unknown flags 0x%x", (unsigned)flags);
+  return divergence_solve(c, f, iters, flags);
 }
 
 DV_API int dv_pressure_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {

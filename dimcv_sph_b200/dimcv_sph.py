@@ -17,7 +17,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED
+from ._abi import (DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED,
+                   DV_SOLVE_NONPRESSURE, DV_SOLVE_PREPARED)
 from .particle_system import Scalar
 
 _MODES = {"bernoulli": DV_SAMPLE_BERNOULLI, "inverse_cdf": DV_SAMPLE_INVERSE_CDF,
@@ -151,7 +152,8 @@ class DIMCVSPHSolver(SPHBase):
 
     # ----------------------------------------------------------- DFSPH
     # Sweeps that the reference runs back to back over the same neighbours
-    # are fused (dv_densities_factor_change, dv_vorticity_dvort): the first
+    # are fused (dv_densities_factor_change, the divergence solve's residual
+    # sweep with the non-pressure forces, dv_vorticity_dvort): the first
     # method computes all the results and a later one skips its sweep while
     # nothing it reads can have changed: no library kernel has run since
     # (the context's launch count) and no tensor it reads was written in place
@@ -161,7 +163,9 @@ class DIMCVSPHSolver(SPHBase):
     _FACTOR_READS = ("x", "m", "m_V", "material")          # compute_DFSPH_factor
     _CHANGE_READS = ("x", "v", "m_V", "material")          # compute_density_change
     _DVORT_READS = ("x", "m_V", "material", "vorticity")   # compute_d_vorticity, with v_star
+    _NONPRESSURE_READS = ("x", "v", "m_V", "material", "is_dynamic")  # compute_non_pressure_forces
     _fused_densities = None
+    _fused_nonpressure = None
     _fused_dvort = None
 
     def _launches(self):
@@ -189,6 +193,8 @@ class DIMCVSPHSolver(SPHBase):
         self._fused_densities = self._fusion_mark(set(self._FACTOR_READS) | set(self._CHANGE_READS))
 
     def compute_non_pressure_forces(self):  # :195-208
+        if self._fusion_fresh(self._fused_nonpressure, self._NONPRESSURE_READS):
+            return  # computed by divergence_solve's last residual sweep, bit-identical
         self._call("dv_nonpressure")
 
     def advect(self):  # :210-218
@@ -235,9 +241,11 @@ class DIMCVSPHSolver(SPHBase):
     def divergence_solve(self):
         """dimcv_sph.py:376-393, with the Jacobi loop on the device."""
         it = C.c_int32(0)
-        fn = "dv_divergence_solve_prepared" if self._fusion_fresh(self._fused_densities, self._CHANGE_READS) \
-            else "dv_divergence_solve"
-        self._call(fn, C.byref(it) if self.track_iterations else None)
+        flags = DV_SOLVE_NONPRESSURE
+        if self._fusion_fresh(self._fused_densities, self._CHANGE_READS):
+            flags |= DV_SOLVE_PREPARED
+        self._call("dv_divergence_solve_ex", flags, C.byref(it) if self.track_iterations else None)
+        self._fused_nonpressure = self._fusion_mark(self._NONPRESSURE_READS)
         self.last_iters = (it.value, self.last_iters[1])
 
     def pressure_solve(self):

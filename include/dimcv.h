@@ -308,6 +308,15 @@ DV_API int dv_divergence_solve(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
  * hold compute_density_change's result for the current v (from
  * dv_densities_factor_change or dv_density_change). */
 DV_API int dv_divergence_solve_prepared(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
+/* dv_divergence_solve with options (flags, OR-ed):
+ *   DV_SOLVE_PREPARED: as dv_divergence_solve_prepared;
+ *   DV_SOLVE_NONPRESSURE: the Jacobi loop's residual sweeps also compute
+ *     compute_non_pressure_forces (dimcv_sph.py:150-208, which the substep
+ *     calls next, karman_vortex.py:236); afterwards acceleration is
+ *     bit-identical to dv_nonpressure on the solved velocity. */
+#define DV_SOLVE_PREPARED 1
+#define DV_SOLVE_NONPRESSURE 2
+DV_API int dv_divergence_solve_ex(dv_ctx* ctx, const dv_fields* f, int32_t flags, int32_t* iters);
 /* DIMCVSPHSolver.pressure_solve (dimcv_sph.py:597-614), same loop form. */
 DV_API int dv_pressure_solve(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
 /* DIMCVSPHSolver.compute_non_pressure_forces (dimcv_sph.py:150-208). */

@@ -490,26 +490,32 @@ def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
     nontrivial(a["density_adv"], "density_adv")
 
     import ctypes
-    solve = ["v", "density_adv", "dfsph_factor"]
+    solve = ["v", "density_adv", "dfsph_factor", "acceleration"]
     for k, t in ps.fields.t.items():
         t.copy_(saved[k])
     it = ctypes.c_int32(0)
     solver._call("dv_densities")
     solver._call("dv_dfsph_factor")
     solver._call("dv_divergence_solve", ctypes.byref(it))
+    solver._call("dv_nonpressure")
     a = snap(solve)
     for k, t in ps.fields.t.items():
         t.copy_(saved[k])
+    ps.acceleration[:n] = float("nan")
     solver.track_iterations = True
     launches = solver._launches()
     solver.compute_densities()
     solver.compute_DFSPH_factor()
     assert solver._launches() == launches + 1  # one sweep for density, factor and density change
     solver.divergence_solve()
+    launches = solver._launches()
+    solver.compute_non_pressure_forces()
+    assert solver._launches() == launches  # from the solve's last residual sweep
     b = snap(solve)
     for k in solve:
         bitexact(b[k], a[k], k)
     assert solver.last_iters[0] == it.value >= 1
+    nontrivial(a["acceleration"], "acceleration")
 
     names = ["solver.v_star", "vorticity", "solver.grad_v", "solver.d_vort"]
     solver._calls("dv_dimcv_vorticity")
@@ -586,6 +592,21 @@ def test_fused_skips_follow_torch_edits(cuda):
     for k in solve:
         bitexact(b[k], a[k], k)
     assert solver.last_iters[0] == it.value
+
+    restore()
+    solver._call("dv_densities")
+    solver._call("dv_dfsph_factor")
+    solver._call("dv_divergence_solve", None)
+    ps.v[:n] *= 0.5
+    solver._call("dv_nonpressure")
+    a = snap(["acceleration"])
+    restore()
+    solver.compute_densities()
+    solver.compute_DFSPH_factor()
+    solver.divergence_solve()
+    ps.v[:n] *= 0.5
+    solver.compute_non_pressure_forces()  # v changed since the solve: computed again
+    bitexact(snap(["acceleration"])["acceleration"], a["acceleration"], "acceleration")
 
     restore()
     solver._call("dv_densities")
