@@ -28,6 +28,7 @@ DV_SAMPLE_STRATIFIED = 3
 
 DV_SOLVE_PREPARED = 1
 DV_SOLVE_NONPRESSURE = 2
+DV_SOLVE_VIS = 4
 
 DV_KERNEL_REF2D = 0
 DV_KERNEL_BLOB3D = 1

@@ -51,6 +51,7 @@ PROTOTYPES = {
     "dv_divergence_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_divergence_solve_prepared": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_divergence_solve_ex": (C.c_int, [_P, _FP, i32, C.POINTER(i32)]),
+    "dv_pressure_solve_ex": (C.c_int, [_P, _FP, _SP, i32, C.POINTER(i32)]),
     "dv_pressure_solve": (C.c_int, [_P, _FP, C.POINTER(i32)]),
     "dv_nonpressure": (C.c_int, [_P, _FP]),
     "dv_predict_velocity": (C.c_int, [_P, _FP]),

@@ -282,6 +282,52 @@ __global__ void k_density_adv(dv_params P, DevGrid G, dv_fields F, const dv_coun
   }
 }
 
+// The pressure solve's opening density_adv sweep and, in the same walk,
+// copy_x_temp + compute_vorticity_vis (dimcv_sph.py:778-801), with the
+// operations and order of k_vis: the vis sweep reads x, m_V, material and
+// vorticity, which the pressure iterations (they write v) leave unchanged, so
+// the solve's first sweep gives what the vis sweep after the solve would.
+template <int D>
+__global__ void k_density_adv_vis(dv_params P, DevGrid G, dv_fields F, dv_solver_fields S,
+                                  const dv_counters* __restrict__ C) {
+  FOR_I;
+  const V3 xi = ldv<D>(F.x, i);
+  stv<D>(S.x_temp, i, xi);
+  if (F.material[i] != DV_MATERIAL_FLUID) {
+    st4(S.vorticity_vis, i, V3{0.f, 0.f, 0.f});
+    return;
+  }
+  const V3 vi = ldv<D>(F.v, i);
+  float delta = 0.0f;
+  const float w = F.m_V[i] * cubic_W(P, 0.0f);
+  const V3 wi = ld4(F.vorticity, i);
+  V3 vort{w * wi.x, w * wi.y, w * wi.z};
+  float ws = w;
+  for_each_neighbor_m<D>(P, G, F.x, F.material, i, xi, [&](int j, V3 r, float r2, int mj) {
+    const float mvj = F.m_V[j];
+    if (mj == DV_MATERIAL_FLUID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      delta += F.m[j] * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+    } else if (mj == DV_MATERIAL_SOLID) {
+      V3 vj = ldv<D>(F.v, j);
+      V3 dv{vi.x - vj.x, vi.y - vj.y, vi.z - vj.z};
+      delta += mvj * P.density0 * dot<D>(dv, cubic_gradW<D>(P, r, r2));
+    }
+    const float wj = mvj * cubic_W(P, sqrtf(r2));
+    const V3 oj = ld4(F.vorticity, j);
+    vort.x += wj * oj.x;
+    vort.y += wj * oj.y;
+    vort.z += wj * oj.z;
+    ws += wj;
+  });
+  float da = F.density[i] + P.dt * delta;
+  da = fmaxf(da, P.density0);
+  F.density_adv[i] = da;
+  const float den = ws + 1e-6f;
+  st4(S.vorticity_vis, i, V3{vort.x / den, vort.y / den, vort.z / den});
+}
+
 // compute_density_error without a preceding sweep (operator surface)
 template <int D>
 __global__ void k_density_error(dv_params P, dv_fields F, const dv_counters* __restrict__ C,
@@ -895,6 +941,28 @@ DV_API int dv_divergence_solve_ex(dv_ctx* c, const dv_fields* f, int32_t flags, 
   if (flags & ~(DV_SOLVE_PREPARED | DV_SOLVE_NONPRESSURE))
     return dv_fail(c, DV_EINVAL, "dv_divergence_solve_ex: unknown flags 0x%x", (unsigned)flags);
   return divergence_solve(c, f, iters, flags);
+}
+
+DV_API int dv_pressure_solve_ex(dv_ctx* c, const dv_fields* f, const dv_solver_fields* s, int32_t flags,
+                                int32_t* iters) {
+  if (!c || !f) return DV_EINVAL;
+  if (flags & ~DV_SOLVE_VIS)
+    return dv_fail(c, DV_EINVAL, "dv_pressure_solve_ex: unknown flags 0x%x", (unsigned)flags);
+  int rc;
+  if (flags & DV_SOLVE_VIS) {
+    if (!s || !s->x_temp || !s->vorticity_vis)
+      return dv_fail(c, DV_EINVAL, "dv_pressure_solve_ex: DV_SOLVE_VIS needs x_temp and vorticity_vis");
+    LAUNCH_D(k_density_adv_vis, nblk(c), c->p, dv_grid(c), *f, *s, c->d_cnt);
+    rc = DV_OK;
+  } else {
+    rc = dv_density_adv(c, f);
+  }
+  if (rc) return rc;
+  rc = dv_scale_factor(c, f, c->p.inv_dt2);
+  if (rc) return rc;
+  rc = jacobi_loop(c, f, 1);
+  if (rc) return rc;
+  return read_iters(c, 1, iters);
 }
 
 DV_API int dv_pressure_solve(dv_ctx* c, const dv_fields* f, int32_t* iters) {

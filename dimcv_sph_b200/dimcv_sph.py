@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from ._abi import (DV_SAMPLE_BERNOULLI, DV_SAMPLE_INJECTED, DV_SAMPLE_INVERSE_CDF, DV_SAMPLE_STRATIFIED,
-                   DV_SOLVE_NONPRESSURE, DV_SOLVE_PREPARED)
+                   DV_SOLVE_NONPRESSURE, DV_SOLVE_PREPARED, DV_SOLVE_VIS)
 from .particle_system import Scalar
 
 _MODES = {"bernoulli": DV_SAMPLE_BERNOULLI, "inverse_cdf": DV_SAMPLE_INVERSE_CDF,
@@ -153,7 +153,8 @@ class DIMCVSPHSolver(SPHBase):
     # ----------------------------------------------------------- DFSPH
     # Sweeps that the reference runs back to back over the same neighbours
     # are fused (dv_densities_factor_change, the divergence solve's residual
-    # sweep with the non-pressure forces, dv_vorticity_dvort): the first
+    # sweep with the non-pressure forces, the pressure solve's opening sweep
+    # with the vis sweep, dv_vorticity_dvort): the first
     # method computes all the results and a later one skips its sweep while
     # nothing it reads can have changed: no library kernel has run since
     # (the context's launch count) and no tensor it reads was written in place
@@ -164,8 +165,10 @@ class DIMCVSPHSolver(SPHBase):
     _CHANGE_READS = ("x", "v", "m_V", "material")          # compute_density_change
     _DVORT_READS = ("x", "m_V", "material", "vorticity")   # compute_d_vorticity, with v_star
     _NONPRESSURE_READS = ("x", "v", "m_V", "material", "is_dynamic")  # compute_non_pressure_forces
+    _VIS_READS = ("x", "m_V", "material", "vorticity")     # copy_x_temp + compute_vorticity_vis
     _fused_densities = None
     _fused_nonpressure = None
+    _fused_vis = None
     _fused_dvort = None
 
     def _launches(self):
@@ -249,12 +252,17 @@ class DIMCVSPHSolver(SPHBase):
         self.last_iters = (it.value, self.last_iters[1])
 
     def pressure_solve(self):
-        """dimcv_sph.py:597-614, with the Jacobi loop on the device."""
+        """dimcv_sph.py:597-614, with the Jacobi loop on the device; when the
+        substep draws the vis fields, its opening sweep computes them too."""
         it = C.c_int32(0)
-        self._call("dv_pressure_solve", C.byref(it) if self.track_iterations else None)
+        flags = DV_SOLVE_VIS if self.compute_vis else 0
+        self._calls("dv_pressure_solve_ex", flags, C.byref(it) if self.track_iterations else None)
+        if flags:
+            self._fused_vis = self._fusion_mark(self._VIS_READS)
         self.last_iters = (self.last_iters[0], it.value)
 
     track_iterations = False
+    compute_vis = False  # KarmanVortexSolver sets it from the scene (computeVis)
 
     # ----------------------------------------------------------- DIMCV
     def compute_v_star(self):  # :264-271 (computed with vorticity and ∇v)
@@ -327,6 +335,8 @@ class DIMCVSPHSolver(SPHBase):
         self._call("dv_life_time")
 
     def copy_x_temp(self):  # :797-801 (with compute_vorticity_vis)
+        if self._fusion_fresh(self._fused_vis, self._VIS_READS):
+            return  # computed by pressure_solve's opening sweep, bit-identical
         self._calls("dv_vis")
 
     def compute_vorticity_vis(self):  # :785-795 — done by copy_x_temp's fused sweep

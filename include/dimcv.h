@@ -319,6 +319,15 @@ DV_API int dv_divergence_solve_prepared(dv_ctx* ctx, const dv_fields* f, int32_t
 DV_API int dv_divergence_solve_ex(dv_ctx* ctx, const dv_fields* f, int32_t flags, int32_t* iters);
 /* DIMCVSPHSolver.pressure_solve (dimcv_sph.py:597-614), same loop form. */
 DV_API int dv_pressure_solve(dv_ctx* ctx, const dv_fields* f, int32_t* iters);
+/* dv_pressure_solve with options (flags):
+ *   DV_SOLVE_VIS: the solve's opening density_adv sweep also does
+ *     copy_x_temp + compute_vorticity_vis (dimcv_sph.py:778-801, which the
+ *     substep calls after the solve, karman_vortex.py:240-241) into s's
+ *     x_temp and vorticity_vis, bit-identical to dv_vis after the solve (the
+ *     iterations write only v, which the vis sweep does not read). */
+#define DV_SOLVE_VIS 4
+DV_API int dv_pressure_solve_ex(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s, int32_t flags,
+                                int32_t* iters);
 /* DIMCVSPHSolver.compute_non_pressure_forces (dimcv_sph.py:150-208). */
 DV_API int dv_nonpressure(dv_ctx* ctx, const dv_fields* f);
 /* DIMCVSPHSolver.predict_velocity (dimcv_sph.py:220-226). */

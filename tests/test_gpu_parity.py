@@ -517,6 +517,30 @@ def test_fused_sweeps_bit_identical_to_separate(cuda, scene):
     assert solver.last_iters[0] == it.value >= 1
     nontrivial(a["acceleration"], "acceleration")
 
+    # the pressure solve's opening sweep with copy_x_temp + compute_vorticity_vis
+    solver._calls("dv_dimcv_vorticity")  # a vorticity for the vis sweep
+    saved = {k: t.clone() for k, t in ps.fields.t.items()}
+    names = ["v", "density_adv", "solver.x_temp", "solver.vorticity_vis"]
+    it = ctypes.c_int32(0)
+    solver._call("dv_pressure_solve", ctypes.byref(it))
+    solver._calls("dv_vis")
+    a = snap(names)
+    for k, t in ps.fields.t.items():
+        t.copy_(saved[k])
+    ps.solver_buf.t["x_temp"].fill_(float("nan"))
+    ps.solver_buf.t["vorticity_vis"].fill_(float("nan"))
+    solver.compute_vis = True
+    solver.pressure_solve()
+    launches = solver._launches()
+    solver.copy_x_temp()
+    solver.compute_vorticity_vis()
+    assert solver._launches() == launches  # from the pressure solve's opening sweep
+    b = snap(names)
+    for k in names:
+        bitexact(b[k], a[k], k)
+    assert solver.last_iters[1] == it.value >= 1
+    nontrivial(a["solver.vorticity_vis"], "vorticity_vis")
+
     names = ["solver.v_star", "vorticity", "solver.grad_v", "solver.d_vort"]
     solver._calls("dv_dimcv_vorticity")
     solver._calls("dv_d_vorticity")
@@ -607,6 +631,20 @@ def test_fused_skips_follow_torch_edits(cuda):
     ps.v[:n] *= 0.5
     solver.compute_non_pressure_forces()  # v changed since the solve: computed again
     bitexact(snap(["acceleration"])["acceleration"], a["acceleration"], "acceleration")
+
+    restore()
+    solver._calls("dv_dimcv_vorticity")
+    saved = {k: t.clone() for k, t in ps.fields.t.items()}
+    solver._call("dv_pressure_solve", None)
+    ps.vorticity[:n] *= 2.0
+    solver._calls("dv_vis")
+    a = snap(["solver.vorticity_vis"])
+    restore()
+    solver.compute_vis = True
+    solver.pressure_solve()
+    ps.vorticity[:n] *= 2.0
+    solver.copy_x_temp()  # vorticity changed since the solve: computed again
+    bitexact(snap(["solver.vorticity_vis"])["solver.vorticity_vis"], a["solver.vorticity_vis"], "vorticity_vis")
 
     restore()
     solver._call("dv_densities")
