@@ -196,8 +196,12 @@ typedef struct dv_ctx dv_ctx;
  * and DIMCVSPHSolver.__init__ (dimcv_sph.py:30-53); field memory stays with
  * the caller.  Returns NULL on failure (message via dv_last_error(NULL)). */
 DV_API dv_ctx* dv_create(const dv_params* params, int64_t capacity, void* stream);
+/* Frees the context's workspace (the caller's fields are not touched). */
 DV_API void dv_destroy(dv_ctx* ctx);
+/* Message of the last failed call on ctx; with NULL, of the calling thread's
+ * last failed dv_create or context-free call. */
 DV_API const char* dv_last_error(const dv_ctx* ctx);
+/* Later calls on ctx run on `stream` (cudaStream_t, NULL = legacy default). */
 DV_API int dv_set_stream(dv_ctx* ctx, void* stream);
 /* Replaces the scalar parameters (time step, tolerances, options) of a live
  * context.  The cell grid (dim, grid_num) must stay the same.  Stands in for
@@ -213,6 +217,7 @@ DV_API int64_t dv_launch_count(const dv_ctx* ctx);
 DV_API int dv_get_counters(dv_ctx* ctx, dv_counters* out);
 /* Sets n / n_fluid / n_solid (after the caller filled fields on its own). */
 DV_API int dv_set_counts(dv_ctx* ctx, int32_t n, int32_t n_fluid, int32_t n_solid);
+/* Clears the sticky DV_WARN_* bits of dv_counters.status. */
 DV_API int dv_clear_status(dv_ctx* ctx);
 
 /* --------------------------------------------------------------- particles */
@@ -482,6 +487,8 @@ DV_API int64_t dv_vpm_workspace_bytes(dv_ctx* ctx, int32_t n, int32_t src_cap, i
  * build (count mismatch, missing lists, capacity). */
 DV_API int dv_vpm_plan_build(dv_ctx* ctx, const dv_fields* f, const dv_solver_fields* s, int32_t mode,
                              dv_vpm_plan* plan);
+/* w_s = ω̃ of w (the smoothing above, dimcv_sph.py:660-677) on the plan's
+ * neighbours; x [n][2], w and w_s [n], in the plan's slot order. */
 DV_API int dv_vpm_smooth(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                          const void* w, void* w_s);
 /* g_w = (∂ω̃/∂ω)^T g_ws, g_x = (∂ω̃/∂x)^T g_ws (written, not accumulated) */
@@ -494,6 +501,9 @@ DV_API int dv_vpm_curl(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, 
 /* g_v = (∂ω/∂v)^T g_w, g_x = (∂ω/∂x)^T g_w (written, not accumulated) */
 DV_API int dv_vpm_curl_bwd(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                            const void* v, const void* g_w, void* g_v, void* g_x);
+/* u = the velocity above (dimcv_sph.py:649-719 without the gate) of w_s on
+ * the plan's neighbours and sources; u [n][2]; workspace of
+ * dv_vpm_workspace_bytes bytes (device). */
 DV_API int dv_vpm_velocity(dv_ctx* ctx, const dv_vpm_plan* plan, int32_t precision, const void* x,
                            const void* w_s, void* u, void* workspace, int64_t workspace_bytes);
 /* g_ws = (∂u/∂ω̃)^T g_u, g_x = (∂u/∂x)^T g_u (written, not accumulated) */
