@@ -276,24 +276,35 @@ __global__ void k_finalize_counts(const int32_t* __restrict__ part, int nparts,
 // so the sweeps do not gather it; a material other than fluid or solid sets
 // bad[0] and the lists are not used.
 //
+// Rows of static solids stay empty: every neighbour walk of the step has a
+// fluid particle (or, for the rigid coupling, a dynamic solid) at its centre,
+// and the static boundary volume (once, at initialisation) scans cells.
+//
 // 3-D (27 cells, ~8 candidates each): one cell-scan pass stores each
 // particle's first `slots` neighbours in its own fixed row and its count; a
 // warp-wide copy then moves the rows into CSR (a particle with more
 // neighbours than slots scans its cells again there).  This saves a second
 // 27-cell scan.  2-D (9 cells): counting is cheap and the fixed rows cost
 // more write traffic than they save, so a count pass and a fill pass.
+__device__ __forceinline__ bool nbr_row_built(const int32_t* __restrict__ mat, const uint8_t* __restrict__ dyn,
+                                              int i) {
+  return !(mat[i] == DV_MATERIAL_SOLID && !dyn[i]);
+}
+
 __device__ __forceinline__ int32_t nbr_entry(int j, int mj, int32_t* bad) {
   if (mj != DV_MATERIAL_FLUID && mj != DV_MATERIAL_SOLID) *bad = 1;
   return (int32_t)((uint32_t)j | (mj == DV_MATERIAL_SOLID ? DV_NBR_SOLID : 0u));
 }
 
 template <int D>
-__global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x,
-                            const dv_counters* __restrict__ C, int m, uint32_t* __restrict__ cnt) {
+__global__ void k_csr_count(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
+                            const uint8_t* __restrict__ dyn, const dv_counters* __restrict__ C, int m,
+                            uint32_t* __restrict__ cnt) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   uint32_t k = 0;
-  if (i < C->n) for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int, V3, float) { ++k; });
+  if (i < C->n && nbr_row_built(mat, dyn, i))
+    for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int, V3, float) { ++k; });
   cnt[i] = k;
 }
 
@@ -301,22 +312,22 @@ template <int D>
 __global__ void k_csr_fill(dv_params P, DevGrid G, const float* __restrict__ x,
                            const int32_t* __restrict__ mat, const dv_counters* __restrict__ C,
                            const uint32_t* __restrict__ off, int32_t* __restrict__ ok,
-                           int32_t* __restrict__ out) {
+                           int32_t* __restrict__ out, const uint8_t* __restrict__ dyn) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C->n || !ok[0]) return;
+  if (i >= C->n || !ok[0] || !nbr_row_built(mat, dyn, i)) return;
   uint32_t k = off[i];
   for_each_neighbor_m<D>(P, G, x, mat, i, ldv<D>(x, i),
                          [&](int j, V3, float, int mj) { out[k++] = nbr_entry(j, mj, ok + 1); });
 }
 
 template <int D>
-__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x,
-                           const dv_counters* __restrict__ C, int m, int slots, uint32_t* __restrict__ cnt,
-                           int32_t* __restrict__ rows) {
+__global__ void k_csr_rows(dv_params P, DevGrid G, const float* __restrict__ x, const int32_t* __restrict__ mat,
+                           const uint8_t* __restrict__ dyn, const dv_counters* __restrict__ C, int m, int slots,
+                           uint32_t* __restrict__ cnt, int32_t* __restrict__ rows) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   uint32_t k = 0;
-  if (i < C->n) {
+  if (i < C->n && nbr_row_built(mat, dyn, i)) {
     int32_t* row = rows + (int64_t)i * slots;
     for_each_neighbor<D>(P, G, x, i, ldv<D>(x, i), [&](int j, V3, float) {
       if (k < (uint32_t)slots) row[k] = j;
@@ -374,10 +385,11 @@ static int build_csr(dv_ctx* c, const dv_fields* f) {
   const bool rows = c->p.dim == 3;
   DV_CK(c, cudaMemsetAsync(c->d_nbr_ok + 1, 0, sizeof(int32_t), c->stream));
   if (rows)
-    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->nbr_slots, c->flags,
-                                                    c->nbr_rows);
+    k_csr_rows<3><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, f->is_dynamic, c->d_cnt, m,
+                                                    c->nbr_slots, c->flags, c->nbr_rows);
   else
-    k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, c->d_cnt, m, c->flags);
+    k_csr_count<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, f->is_dynamic, c->d_cnt, m,
+                                                     c->flags);
   DV_LAUNCHED(c);
   int rc = dv_scan_u32(c, c->flags, c->nbr_off, m);
   if (rc) return rc;
@@ -388,7 +400,7 @@ static int build_csr(dv_ctx* c, const dv_fields* f) {
                                                        c->nbr_rows, c->nbr_off, c->d_nbr_ok, c->nbr_idx);
   else
     k_csr_fill<2><<<nb, DV_THREADS, 0, c->stream>>>(c->p, G, f->x, f->material, c->d_cnt, c->nbr_off,
-                                                    c->d_nbr_ok, c->nbr_idx);
+                                                    c->d_nbr_ok, c->nbr_idx, f->is_dynamic);
   DV_LAUNCHED(c);
   k_csr_material_check<<<1, 1, 0, c->stream>>>(c->d_nbr_ok);
   DV_LAUNCHED(c);

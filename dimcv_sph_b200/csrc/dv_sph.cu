@@ -670,7 +670,8 @@ static inline int nblk(const dv_ctx* c) { return dv_blocks(std::min<int64_t>(c->
 
 DV_API int dv_boundary_volume(dv_ctx* c, const dv_fields* f) {
   if (!c || !f) return DV_EINVAL;
-  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid(c), *f, c->d_cnt, 0);
+  // the stored lists leave static solids' rows empty: scan cells
+  LAUNCH_D(k_boundary_volume, nblk(c), c->p, dv_grid_cells(c), *f, c->d_cnt, 0);
   return DV_OK;
 }
 

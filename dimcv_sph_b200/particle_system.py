@@ -340,7 +340,8 @@ class ParticleSystem:
 
     def stored_neighbor_lists(self):
         """The lists the sweeps read, as the last grid build stored them:
-        (offsets int64 [n+1], neighbours int32 [pairs]) on the device."""
+        (offsets int64 [n+1], neighbours int32 [pairs]) on the device.  Rows
+        of static solids are empty (no sweep of the step walks them)."""
         n = self.particle_num[None]
         off = torch.zeros(n + 1, dtype=torch.int32, device=self.device)
         total = self.lib.dv_stored_lists(self.ctx, C.c_void_p(off.data_ptr()), None, 0)

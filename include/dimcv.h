@@ -257,7 +257,9 @@ DV_API int64_t dv_neighbor_lists(dv_ctx* ctx, const dv_fields* f, int64_t* offse
                                  int32_t* nbrs, int64_t max_pairs);
 /* New (checking): the neighbour lists the sweeps read, as the last grid build
  * (dv_grid_build) stored them: CSR offsets (n+1 uint32) and entries in visit
- * order, copied into device buffers (either may be NULL; call with
+ * order, copied into device buffers.  Rows of static solids are empty: no
+ * sweep of the step walks them (dv_neighbor_lists has every row).  Either
+ * buffer may be NULL; call with
  * nbrs = NULL first to learn the entry count).  Returns the entry count, or a
  * negative dv_status: DV_EINVAL when no valid lists are stored (positions
  * or the particle count changed since the build, or they did not fit),

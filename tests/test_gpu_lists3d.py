@@ -23,23 +23,32 @@ def oracle_lists(ps):
 
 
 def check_stored(ps):
+    """Every row the step walks (fluid and dynamic solids) equals the
+    oracle's; the rows of static solids are stored empty.  The cell-scan
+    export has every row and equals the oracle."""
     off, nbr = (t.cpu().numpy() for t in ps.stored_neighbor_lists())
     ooff, onbr = oracle_lists(ps)
-    assert np.array_equal(off, ooff), "offsets"
-    assert np.array_equal(nbr, onbr), "entries"
-    # the cell-scan export agrees too
+    n = ooff.size - 1
+    snap = ps.snapshot()
+    static = (snap["material"][:n] == 0) & (snap["is_dynamic"][:n] == 0)
+    cnt, ocnt = np.diff(off), np.diff(ooff)
+    assert np.all(cnt[static] == 0), "static solid rows"
+    assert np.array_equal(cnt[~static], ocnt[~static]), "row lengths"
+    keep = np.repeat(~static, ocnt)
+    assert np.array_equal(nbr, onbr[keep]), "entries"
     eoff, enbr = (t.cpu().numpy() for t in ps.neighbor_lists())
-    assert np.array_equal(eoff, off) and np.array_equal(enbr, nbr)
-    return off
+    assert np.array_equal(eoff, ooff) and np.array_equal(enbr, onbr)
+    return ooff, static
 
 
 def test_sphere_scene_lists(cuda):
     from dimcv_sph_b200.particle_system import ParticleSystem
     ps = ParticleSystem(scenes.sphere3d(radius=0.016, dt=6.4e-4))
     ps.initialize_particle_system()
-    off = check_stored(ps)
+    off, static = check_stored(ps)
     c = np.diff(off)
     assert ps.counters()["n"] > 40000 and c.max() <= 64 and c.mean() > 20
+    assert static.sum() > 1000  # the sphere and the walls
 
 
 def box3d(reserved):
@@ -71,5 +80,5 @@ def test_dense_block_crowded_particle_and_clamped_solid(cuda):
     add(ps, [[1.3, 0.5, 0.5], [0.97, 0.5, 0.5]], 0)
     ps.initialize_particle_system()
     assert ps.counters()["status"] & 4  # a particle outside the grid
-    off = check_stored(ps)
+    off, _ = check_stored(ps)
     assert np.diff(off).max() > 64
