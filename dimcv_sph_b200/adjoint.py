@@ -31,7 +31,6 @@ because every kernel of the pipeline is deterministic.
 from __future__ import annotations
 
 import ctypes as C
-import math
 import time
 
 import numpy as np

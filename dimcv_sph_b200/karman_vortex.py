@@ -9,7 +9,6 @@ from pathlib import Path
 import numpy as np
 import torch
 
-from ._abi import MATERIAL_FLUID
 from .dimcv_sph import DIMCVSPHSolver
 
 
