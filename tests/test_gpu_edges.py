@@ -197,3 +197,22 @@ def test_particle_with_more_neighbours_than_list_slots(cuda):
     solver.compute_non_pressure_forces()
     o.call("nonpressure")
     assert np.array_equal(ps.snapshot()["acceleration"], o.snapshot()["acceleration"])
+
+
+def test_unknown_solve_flags_are_errors(cuda):
+    """dv_divergence_solve_ex and dv_pressure_solve_ex refuse flags they do not
+    know, and DV_SOLVE_VIS without the solver fields, before launching anything."""
+    from dimcv_sph_b200._abi import DV_EINVAL, DV_SOLVE_NONPRESSURE, DV_SOLVE_VIS
+    from dimcv_sph_b200.dimcv_sph import DIMCVSPHSolver
+    from dimcv_sph_b200.particle_system import ParticleSystem
+    ps = ParticleSystem(box_cfg(2, reserved=64))
+    solver = DIMCVSPHSolver(ps)
+    lib, ctx, f = ps.lib, ps.ctx, C.byref(ps.fields_struct)
+    launches = solver._launches()
+    assert lib.dv_divergence_solve_ex(ctx, f, 8, None) == DV_EINVAL
+    assert b"flags" in lib.dv_last_error(ctx)
+    assert lib.dv_divergence_solve_ex(ctx, f, DV_SOLVE_VIS, None) == DV_EINVAL
+    assert lib.dv_pressure_solve_ex(ctx, f, C.byref(ps.solver_buf.struct), DV_SOLVE_NONPRESSURE, None) == DV_EINVAL
+    assert lib.dv_pressure_solve_ex(ctx, f, None, DV_SOLVE_VIS, None) == DV_EINVAL
+    assert b"x_temp" in lib.dv_last_error(ctx)
+    assert solver._launches() == launches
