@@ -41,7 +41,7 @@ FLOPS_PER_PAIR_BLOB = 27
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)  # the sphere configuration's 100 steps
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["sphere3d", "channel2d"], default="sphere3d")
